@@ -1,0 +1,303 @@
+"""Throughput of the fused WCA flood step on B200.
+
+Workload: a 4096 x 4096 grid at 90 m (16.8 M LAND
+cells), fBm relief of 20 m amplitude, six Manning classes, 30 mm/h rain for
+2 h and a north-edge point inflow (triangle peaking at 500 m^3/s at 3 h),
+open south edge. A "step" is one WCA step over the whole grid. The timed
+steps start from a warm state: 20 mm of water on every cell (what 40 minutes
+of the storm leaves), as the reference's benchmarks start from a warm start.
+Inputs are far larger than L2 (about 420 MB touched per step), so no L2
+flush is needed between steps.
+
+Metric: Gcell-updates/s = LAND cells x steps / time (the reference's mcups,
+src/common/log.c:133-135). `value` is timed on the device with CUDA events
+around K steps on the session stream; `e2e` is a whole config-2 run (6 h
+simulated) through the reference-facing fca_cuda_run C-ABI with host
+buffers, host<->device copies included. `cpu_baseline` is the reference's
+own OpenMP core (compiled from its sources with its release flags) on a
+bounded sample of the same workload on this host's cores.
+
+--impl reference times that reference CPU implementation alone.
+Multi-GPU: independent replicas, one per rank (the single-domain path has no
+exchange step); value is the whole-job aggregate, max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-updates/s"
+BYTES_PER_CELL = 25  # read z, h, n, hmax (4 B each) + mask (1 B); write h, hmax (4 B each)
+
+
+def warm_domain(n: int):
+    from floodca_b200 import synth
+    dom, p = synth.config2(n=n)
+    dom = dom.copy()
+    dom.h = np.full(dom.shape, 0.02, np.float32)
+    dom.hmax = dom.h.copy()
+    return dom, p
+
+
+def measured_peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per k_step launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "k_step_traffic.json"
+    try:
+        return float(json.loads(f.read_text())["dram_bytes_per_launch_4096"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples taken while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.rows.append([x.strip() for x in ln.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8
+                          for i, v in enumerate(r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU implementation (the OpenMP core compiled in oracle/_ref).
+
+def reference_cpu(dom, p, steps: int, warmup: int, budget_s: float) -> dict:
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    from oracle import refcore
+    from floodca_b200.sim import Domain
+    kind = refcore.shipped_kind()
+    if not refcore.available(kind):
+        return {"unavailable": f"oracle/_ref/libfcaref_{kind}.so missing (reference not built)"}
+    # time one step on the full grid to size the sample within the budget
+    run = refcore.RefRun(dom, p.with_(steps=0, T_sim=1e7), kind)
+    t0 = time.perf_counter()
+    run.step()
+    t1 = time.perf_counter() - t0
+    nr = dom.shape[0]
+    rows = nr
+    if t1 * (steps + warmup) > budget_s:
+        rows = max(64, int(nr * budget_s / (t1 * (steps + warmup))))
+    if rows < nr:
+        sl = slice(0, rows)
+        dom = Domain(z=dom.z[sl], mask=dom.mask[sl], n=dom.n[sl], C=dom.C[sl], Rday=dom.Rday[sl],
+                     h=dom.h[sl], dx=dom.dx, hmax=dom.hmax[sl], tmax=None)
+        run = refcore.RefRun(dom, p.with_(steps=0, T_sim=1e7), kind)
+    for _ in range(warmup):
+        run.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run.step()
+    wall = time.perf_counter() - t0
+    cells = int((dom.mask == 0).sum())
+    return {"value": cells * steps / wall / 1e9, "cores": threads, "kind": "reference",
+            "sample": f"{rows}x{dom.shape[1]} rows of the warm 4096^2 config-2 grid, {steps} steps "
+                      f"after {warmup} warm-up, libfcaref_{kind} (reference src/common, -O3 "
+                      f"{'-march=x86-64-v4' if kind.endswith('v4') else '-march=x86-64-v3'}, OpenMP)",
+            "wall_s": wall, "steps": steps, "cells": cells}
+
+
+def line_reference(args, n: int) -> dict:
+    dom, p = warm_domain(n)
+    r = reference_cpu(dom, p, args.steps, args.warmup, args.cpu_budget)
+    base = {"metric": METRIC, "impl": "reference", "unit": "Gcell/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_block(n, args.gpus)}
+    if "unavailable" in r:
+        return {"impl": "reference", "unavailable": r["unavailable"]}
+    base.update(value=r["value"], ms_per_step=1e3 * r["wall_s"] / r["steps"],
+                cpu_baseline={"value": r["value"], "unit": "Gcell/s", "cores": r["cores"],
+                              "kind": "reference", "sample": r["sample"]},
+                e2e={"value": r["value"], "unit": "Gcell/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
+    return base
+
+
+def config_block(n: int, gpus: int) -> dict:
+    return {"workload": f"config-2 single domain {n}x{n}, 90 m, point inflow + 30 mm/h rain, "
+                        "open south edge, warm start (20 mm), FP32 stencil / FP64 accumulation",
+            "grid": [n, n], "K": 4, "U": 1, "precision": "f32-exact",
+            "parallelism": f"replicas x{gpus}" if gpus > 1 else "single GPU",
+            "l2": "inputs (~420 MB per step) larger than L2; no flush"}
+
+
+# ---------------------------------------------------------------------------
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--math", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--cpl", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds of CPU time for the reference baseline sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = args.size
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(line_reference(args, n)), flush=True)
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    from floodca_b200.sim import DropinGrid, Session
+
+    dom, p = warm_domain(n)
+    # keep the run going for all W+K steps (events of the storm still apply)
+    pb = p.with_(T_sim=30 * 86400.0)
+    sess = Session(dom, pb, precision="f32", math=args.math, cols_per_lane=args.cpl)
+    info = sess.info()
+    land = info["land_cells"]
+    stream = torch.cuda.ExternalStream(sess.stream())
+    sess.advance(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    l0 = sess.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sess.advance(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+    launches = sess.launches() - l0
+    ms = e0.elapsed_time(e1)
+    st = sess.stats()
+    active = st["step"] == args.warmup + args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    sess.close()
+
+    value = world * land * args.steps / (ms / 1e3) / 1e9
+    per_launch_s = ms / 1e3 / args.steps
+    alg_bytes = BYTES_PER_CELL * land
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs")
+    achieved = alg_bytes / per_launch_s / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak or 6650.0, "unit": "GB/s",
+            "frac": achieved / (peak or 6650.0), "traffic": profile_traffic(),
+            "peak_source": "measured" if peak else "fallback",
+            "bytes_per_cell": BYTES_PER_CELL, "kernel": "k_step"}
+
+    out = {"metric": METRIC, "value": value, "unit": "Gcell/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": config_block(n, world), "roofline": roof,
+           "clocks": clk.summary(), "gpu_launches": int(launches),
+           "all_steps_active": bool(active), "launch": info, "math": args.math}
+
+    if not args.no_e2e:
+        dom2, p2 = __import__("floodca_b200.synth", fromlist=["config2"]).config2(n=n)
+        g = DropinGrid(dom2, p2)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        rc = g.run()
+        wall = time.perf_counter() - t0
+        res = g.result()
+        if world > 1:
+            t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        steps = res["step"]
+        es = 4 * 7 + 1  # z h n C Rday hmax tmax (f32) + mask per cell
+        out["e2e"] = {"value": world * land * steps / wall / 1e9, "unit": "Gcell/s",
+                      "h2d_bytes_per_step": es * n * n / max(steps, 1),
+                      "d2h_bytes_per_step": 12 * n * n / max(steps, 1),
+                      "api": "fca_cuda_run (host buffers)", "run": "config 2, 6 h simulated",
+                      "steps": steps, "wall_s": wall, "rc": rc, "E_mass": None}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = reference_cpu(dom, p, 5, 1, args.cpu_budget)
+        if "unavailable" not in r:
+            out["cpu_baseline"] = {"value": r["value"], "unit": "Gcell/s", "cores": r["cores"],
+                                   "kind": r["kind"], "sample": r["sample"]}
+        else:
+            out["cpu_baseline"] = r
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,82 @@
+// Kernel variant table shared by the session code and the per-precision
+// instantiation units (wca_inst_*.cu), so the variants compile in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "wca_kernels.cuh"
+
+namespace fcab {
+
+// Selects one compiled step-kernel variant.
+struct VariantKey {
+    int prec;   // FCAB_PREC_*
+    int K;      // 4 or 8
+    int cpl;    // 1, 2 or 4
+    int math;   // MATH_*
+    int rainf;  // per-cell rain field
+};
+
+// Type-erased launchers; `g`, `rk` point at GridD<T>/RunK<T> of the variant's T.
+struct Launchers {
+    cudaError_t (*step)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
+                        int warps_total, int grid, cudaStream_t s);
+    cudaError_t (*init)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl, int grid,
+                        cudaStream_t s);
+    const void *step_fn;   // __global__ symbol, for occupancy queries
+};
+
+// Returns false when the variant is not compiled.
+bool lookup_f32(const VariantKey &k, Launchers *out);
+bool lookup_f32all(const VariantKey &k, Launchers *out);
+bool lookup_f64(const VariantKey &k, Launchers *out);
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+cudaError_t launch_step(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
+                        int warps_total, int grid, cudaStream_t s)
+{
+    k_step<T, AccT, K, CPL, MATH, RAINF><<<grid, 128, 0, s>>>(
+        *static_cast<const GridD<T> *>(g), *static_cast<const RunK<T> *>(rk), tc, ctl,
+        warps_total);
+    return cudaGetLastError();
+}
+
+template <typename T, int K, int MATH>
+cudaError_t launch_init(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl, int grid,
+                        cudaStream_t s)
+{
+    k_init_dt<T, K, MATH><<<grid, 256, 0, s>>>(*static_cast<const GridD<T> *>(g),
+                                              *static_cast<const RunK<T> *>(rk), tc, ctl);
+    return cudaGetLastError();
+}
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+Launchers make_launchers()
+{
+    Launchers L;
+    L.step = &launch_step<T, AccT, K, CPL, MATH, RAINF>;
+    L.init = &launch_init<T, K, MATH>;
+    L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF>;
+    return L;
+}
+
+// Expands the (K, CPL, RAINF) combinations for one (T, AccT, MATH).
+template <typename T, typename AccT, int MATH>
+bool lookup_kcr(const VariantKey &k, Launchers *out)
+{
+#define FCAB_CASE(KK, CC, RR)                                                    \
+    if (k.K == KK && k.cpl == CC && (k.rainf != 0) == RR) {                      \
+        *out = make_launchers<T, AccT, KK, CC, MATH, RR>();                     \
+        return true;                                                             \
+    }
+    FCAB_CASE(4, 1, false) FCAB_CASE(4, 1, true)
+    FCAB_CASE(4, 2, false) FCAB_CASE(4, 2, true)
+    FCAB_CASE(4, 4, false) FCAB_CASE(4, 4, true)
+    FCAB_CASE(8, 1, false) FCAB_CASE(8, 1, true)
+    FCAB_CASE(8, 2, false) FCAB_CASE(8, 2, true)
+    FCAB_CASE(8, 4, false) FCAB_CASE(8, 4, true)
+#undef FCAB_CASE
+    return false;
+}
+
+}  // namespace fcab

@@ -1,0 +1,979 @@
+// Fused WCA step kernel for sm_100a.
+//
+// One launch = one step of FloodCA's fca_step (src/common/model.c:321-605)
+// over the whole grid, with the next step's stable-dt reduction
+// (model.c:111-156) fused in and all step control (dt clamp, event clamp,
+// hyetograph integral, time advance; model.c:363-382, 600-601,
+// src/common/rain.c:30-93) kept on the device, so the host never waits
+// inside a run.
+//
+// Work decomposition: a warp streams down a vertical strip of 32*CPL columns
+// (lane l holds CPL adjacent columns), one input row per iteration, through a
+// register pipeline:
+//   iteration i loads row i+1 (prefetch) and computes
+//     A  x-face discharge of row i and y-face (and diagonal) discharge
+//        between rows i-1 and i              (physics.h:51-125)
+//     C  outflow sum and limiter s of row i-1  (model.c:489-502)
+//     D  limiter-scaled net inflow, rain, clamp, hmax/tmax of row i-2
+//        (model.c:511-597); the row is written if it is an output row
+//     E  the next step's per-cell stable velocity of row i-3 from the new
+//        depths of rows i-4..i-2 (physics.h:158-217)
+// Horizontal neighbours come from the adjacent lane by warp shuffle. A strip
+// overlaps its neighbours by HL columns on each side (3 halo columns are
+// needed: E at column c needs new depth at c+-1, which needs s at c+-2,
+// which needs fluxes reaching c+-3), so only its middle OW columns are
+// written. Every warp owns a contiguous, balanced range of (strip, row)
+// pairs; the vertical halo costs 6 pipeline iterations per segment.
+//
+// The minimum over cells of alpha*dx/v equals alpha*dx / max(v) (division by
+// a positive number rounds monotonically), so warps reduce max(v) and
+// publish it with one atomicMax on the float bit pattern. The last CTA to
+// finish prepares the next step's control block.
+#pragma once
+
+#include "wca_physics.cuh"
+
+namespace fcab {
+
+constexpr int PADR = 4;   // padded rows above and below the grid
+constexpr int PADC = 4;   // padded columns left of the grid
+constexpr int NSLOT = 32; // accumulator slots (spread the atomics)
+
+template <int CPL>
+struct Geom {
+    static constexpr int HL = CPL == 1 ? 3 : 4;     // halo columns each side
+    static constexpr int SW = 32 * CPL;             // strip width (columns)
+    static constexpr int OW = SW - 2 * HL;          // output columns per strip
+};
+
+// Device view of the padded grid. Element (r, c) of the nrows x ncols grid is
+// at index (r + PADR) * pitch + (c + PADC); padding cells are WALL with zero
+// z, h and n.
+template <typename T>
+struct GridD {
+    const T *z, *n, *cr;        // cr: per-cell C*Rday, or nullptr
+    const uint8_t *m;
+    T *h0, *h1, *hmax, *tmax;
+    long long pitch;
+    int nr, nc;
+};
+
+// Uniform run constants.
+template <typename T>
+struct RunK {
+    StepK<T> k;                 // dt-independent members filled
+    T dt_max, dt_min, cr_uniform;
+    int K, U, open, edge_n, edge_s, edge_w, edge_e;
+    int inflow_r, inflow_c;     // -1: none
+    int has_sea;
+};
+
+// Host-visible control block; one per run, in device memory.
+struct Ctl {
+    // prepared for the next step by the previous step's last CTA
+    double t, dt, F, tmax_val, inflow_dh, t_next, dt_base;
+    int step, hit, active, h_cur, want_v, done, pause, force_day;
+    int err, n_force_days, pad0, pad1;
+    long long dt_min_hits;
+    unsigned long long vmax_bits;
+    unsigned int ctas_done;
+    unsigned int launches;
+    double V_in;                // inflow volume added by the steps taken
+    double V_in_step;           // inflow volume of the prepared step
+    double accd[4][NSLOT];      // V_rain, clamp, V_sea, V_bnd (double accumulation)
+    float accf[4][NSLOT];       // same, FP32 accumulation
+    unsigned long long cap[NSLOT];
+};
+
+// Event and forcing parameters for the device-side step control.
+struct TimeCfg {
+    double T_sim, out_every, D_h, phi, rain_end;
+    double inflow_peak, inflow_t_peak, inflow_t_end;
+    double alpha_dx_d;
+    int hyeto, max_steps, U, time_f32;
+    int n_force_days, progress_every, inflow_ok, prec_f64;
+};
+
+// --------------------------------------------------------------------------
+// Step control (device, one thread): FloodCA src/common/rain.c:8-93 and the
+// loop of src/common/model.c:607-643.
+
+__device__ __forceinline__ double tri_f(double t, double T, double tp)
+{
+    if (t < 0.0 || t >= T || T <= 0.0)
+        return 0.0;
+    if (t < tp)
+        return tp <= 0.0 ? 0.0 : (2.0 / T) * (t / tp);
+    return T - tp <= 0.0 ? 0.0 : (2.0 / T) * ((T - t) / (T - tp));
+}
+
+__device__ inline double hyeto_integral(const TimeCfg &c, double t, double dt)
+{
+    if (dt <= 0.0)
+        return 0.0;
+    double t1 = t + dt;
+    if (c.hyeto == 1)
+        return dt / 86400.0;
+    double T = c.D_h * 3600.0, tp = c.phi * T, sum = 0.0, a;
+    if (t1 <= 0.0 || t >= T)
+        return 0.0;
+    if (t < 0.0)
+        t = 0.0;
+    if (t1 > T)
+        t1 = T;
+    a = t;
+    for (int guard = 0; a < t1 - 1e-15 && guard < 4; guard++) {
+        double b = (a < tp && t1 > tp) ? tp : t1;
+        sum += 0.5 * (tri_f(a, T, tp) + tri_f(b, T, tp)) * (b - a);
+        a = b;
+    }
+    return sum;
+}
+
+__device__ inline double next_event(const TimeCfg &c, double t)
+{
+    double t_next = c.T_sim;
+    double t_day = (floor(t / 86400.0) + 1.0) * 86400.0;
+    if (t_day - t < 1e-9)
+        t_day += 86400.0;
+    if (t_day < t_next)
+        t_next = t_day;
+    if (c.out_every > 0.0) {
+        double t_out = (floor(t / c.out_every) + 1.0) * c.out_every;
+        if (t_out - t < 1e-9)
+            t_out += c.out_every;
+        if (t_out < t_next)
+            t_next = t_out;
+    }
+    if (c.rain_end > 0.0 && c.rain_end - t >= 1e-9 && c.rain_end < t_next)
+        t_next = c.rain_end;
+    return t_next;
+}
+
+__device__ inline double inflow_rate(const TimeCfg &c, double t)
+{
+    if (t <= 0.0 || t >= c.inflow_t_end)
+        return 0.0;
+    if (t <= c.inflow_t_peak)
+        return c.inflow_t_peak > 0.0 ? c.inflow_peak * (t / c.inflow_t_peak) : c.inflow_peak;
+    return c.inflow_t_end > c.inflow_t_peak
+               ? c.inflow_peak * ((c.inflow_t_end - t) / (c.inflow_t_end - c.inflow_t_peak))
+               : 0.0;
+}
+
+__device__ inline double inflow_volume(const TimeCfg &c, double t, double dt)
+{
+    if (!c.inflow_ok || dt <= 0.0)
+        return 0.0;
+    double t1 = t + dt, a, sum = 0.0;
+    if (t < 0.0)
+        t = 0.0;
+    if (t1 > c.inflow_t_end)
+        t1 = c.inflow_t_end;
+    a = t;
+    for (int guard = 0; a < t1 && guard < 4; guard++) {
+        double b = (a < c.inflow_t_peak && t1 > c.inflow_t_peak) ? c.inflow_t_peak : t1;
+        sum += 0.5 * (inflow_rate(c, a) + inflow_rate(c, b)) * (b - a);
+        a = b;
+    }
+    return sum;
+}
+
+// Prepares ctl for the step after the one just taken (after_step) or for
+// the first step. Runs on one thread once every CTA's atomics are visible.
+template <typename T>
+__device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool after_step)
+{
+    double t = c->t;
+    int step = c->step;
+    if (after_step) {
+        if (c->hit)
+            t = c->t_next;
+        else if (tc.time_f32)
+            t = (double)((float)c->t + (float)c->dt);
+        else
+            t = c->t + c->dt;
+        step += 1;
+        c->V_in += c->V_in_step;
+    }
+    bool done = tc.max_steps > 0 ? step >= tc.max_steps : t >= tc.T_sim - 1e-15;
+    int pause = 0;
+    if (!done && tc.n_force_days > 0) {
+        int d = t < 0.0 ? 0 : (int)floor(t / 86400.0);
+        if (d >= tc.n_force_days)
+            d = tc.n_force_days - 1;
+        if (d != c->force_day)
+            pause = 1;              // the host loads the day's Rday, then resumes
+    }
+    if (!done && after_step && tc.progress_every > 0 && step % tc.progress_every == 0)
+        pause = 1;
+    T dt_base = (T)c->dt_base;
+    if (!done && step % tc.U == 0) {
+        T vmax;
+        if (sizeof(T) == 4)
+            vmax = (T)__uint_as_float((unsigned)c->vmax_bits);
+        else
+            vmax = (T)__longlong_as_double((long long)c->vmax_bits);
+        T dtm = rk.dt_max;
+        if (vmax > T(0)) {
+            T dta = rk.k.alpha_dx / vmax;
+            if (dta < dtm)
+                dtm = dta;
+        }
+        if (dtm < rk.dt_min) {
+            dtm = rk.dt_min;
+            c->dt_min_hits += 1;
+        }
+        if (dtm > rk.dt_max)
+            dtm = rk.dt_max;
+        dt_base = dtm;
+    }
+    T dt = dt_base;
+    double t_next = 0.0;
+    int hit = 0;
+    double F = 0.0, V_in = 0.0;
+    if (!done) {
+        t_next = next_event(tc, t);
+        double remain = t_next - t;
+        if (remain <= (double)dt) {
+            if (remain < 0.0)
+                remain = 0.0;
+            dt = (T)remain;
+            hit = 1;
+        }
+        if (!(dt > T(0)))
+            done = true;            // the reference loop stops advancing here
+    }
+    if (!done) {
+        bool rain_on = tc.rain_end <= 0.0 || tc.rain_end - t >= 1e-9;
+        F = rain_on ? hyeto_integral(tc, t, (double)dt) : 0.0;
+        V_in = inflow_volume(tc, t, (double)dt);
+    }
+    c->t = t;
+    c->step = step;
+    c->dt_base = (double)dt_base;
+    c->dt = (double)dt;
+    c->t_next = t_next;
+    c->hit = hit;
+    c->F = F;
+    c->inflow_dh = (double)(T)(V_in / (double)rk.k.A);
+    c->V_in_step = V_in;
+    if (tc.time_f32)
+        c->tmax_val = (double)((float)t + (float)dt);
+    else
+        c->tmax_val = t + (double)dt;
+    c->want_v = (step + 1) % tc.U == 0;
+    c->done = done ? 1 : 0;
+    c->pause = pause;
+    c->active = (!done && !pause) ? 1 : 0;
+    c->vmax_bits = 0ull;
+    c->ctas_done = 0u;
+}
+
+// --------------------------------------------------------------------------
+// Row loads (vectorised by CPL).
+
+template <typename T, int CPL>
+struct VecIO;
+
+template <int CPL>
+struct VecIO<float, CPL> {
+    static __device__ __forceinline__ void ld(float (&x)[CPL], const float *p)
+    {
+        if constexpr (CPL == 4) {
+            float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+            x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+        } else if constexpr (CPL == 2) {
+            float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+            x[0] = v.x; x[1] = v.y;
+        } else {
+            x[0] = __ldg(p);
+        }
+    }
+    static __device__ __forceinline__ void ld_rw(float (&x)[CPL], const float *p)
+    {
+        if constexpr (CPL == 4) {
+            float4 v = *reinterpret_cast<const float4 *>(p);
+            x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+        } else if constexpr (CPL == 2) {
+            float2 v = *reinterpret_cast<const float2 *>(p);
+            x[0] = v.x; x[1] = v.y;
+        } else {
+            x[0] = *p;
+        }
+    }
+    static __device__ __forceinline__ void st(float *p, const float (&x)[CPL])
+    {
+        if constexpr (CPL == 4)
+            *reinterpret_cast<float4 *>(p) = make_float4(x[0], x[1], x[2], x[3]);
+        else if constexpr (CPL == 2)
+            *reinterpret_cast<float2 *>(p) = make_float2(x[0], x[1]);
+        else
+            *p = x[0];
+    }
+};
+
+template <int CPL>
+struct VecIO<double, CPL> {
+    static __device__ __forceinline__ void ld(double (&x)[CPL], const double *p)
+    {
+#pragma unroll
+        for (int j = 0; j < CPL; j += (CPL >= 2 ? 2 : 1)) {
+            if constexpr (CPL >= 2) {
+                double2 v = __ldg(reinterpret_cast<const double2 *>(p + j));
+                x[j] = v.x;
+                x[j + 1] = v.y;
+            } else {
+                x[j] = __ldg(p + j);
+            }
+        }
+    }
+    static __device__ __forceinline__ void ld_rw(double (&x)[CPL], const double *p)
+    {
+#pragma unroll
+        for (int j = 0; j < CPL; j++)
+            x[j] = p[j];
+    }
+    static __device__ __forceinline__ void st(double *p, const double (&x)[CPL])
+    {
+#pragma unroll
+        for (int j = 0; j < CPL; j += (CPL >= 2 ? 2 : 1)) {
+            if constexpr (CPL >= 2)
+                *reinterpret_cast<double2 *>(p + j) = make_double2(x[j], x[j + 1]);
+            else
+                p[j] = x[j];
+        }
+    }
+};
+
+template <int CPL>
+__device__ __forceinline__ void ld_mask(uint32_t (&m)[CPL], const uint8_t *p)
+{
+    if constexpr (CPL == 4) {
+        uint32_t v = __ldg(reinterpret_cast<const unsigned int *>(p));
+        m[0] = v & 0xffu; m[1] = (v >> 8) & 0xffu; m[2] = (v >> 16) & 0xffu; m[3] = v >> 24;
+    } else if constexpr (CPL == 2) {
+        uint32_t v = __ldg(reinterpret_cast<const unsigned short *>(p));
+        m[0] = v & 0xffu; m[1] = v >> 8;
+    } else {
+        m[0] = __ldg(p);
+    }
+}
+
+template <typename T, int CPL>
+struct Row {
+    T z[CPL], h[CPL], n[CPL];
+    uint32_t m[CPL];
+};
+
+template <typename T, int CPL>
+__device__ __forceinline__ void load_row(Row<T, CPL> &R, const GridD<T> &g, const T *hin,
+                                         long long off)
+{
+    VecIO<T, CPL>::ld(R.z, g.z + off);
+    VecIO<T, CPL>::ld(R.h, hin + off);
+    VecIO<T, CPL>::ld(R.n, g.n + off);
+    ld_mask<CPL>(R.m, g.m + off);
+}
+
+template <typename T>
+__device__ __forceinline__ T sh_dn(T v)
+{
+    return __shfl_down_sync(0xffffffffu, v, 1);
+}
+template <typename T>
+__device__ __forceinline__ T sh_up(T v)
+{
+    return __shfl_up_sync(0xffffffffu, v, 1);
+}
+
+// Right / left neighbour of the lane's column j within a row held as CPL
+// values per lane.
+template <typename T, int CPL>
+__device__ __forceinline__ T right_of(const T (&x)[CPL], int j, T nxt0)
+{
+    return j + 1 < CPL ? x[j + 1 < CPL ? j + 1 : 0] : nxt0;
+}
+template <typename T, int CPL>
+__device__ __forceinline__ T left_of(const T (&x)[CPL], int j, T prv_last)
+{
+    return j > 0 ? x[j > 0 ? j - 1 : 0] : prv_last;
+}
+
+template <typename A>
+__device__ __forceinline__ A warp_sum(A v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// --------------------------------------------------------------------------
+// The step kernel.
+
+template <typename T>
+__device__ __forceinline__ T qnan_of();
+template <>
+__device__ __forceinline__ float qnan_of<float>()
+{
+    return __int_as_float(0x7fc00000);
+}
+template <>
+__device__ __forceinline__ double qnan_of<double>()
+{
+    return __longlong_as_double(0x7ff8000000000000ll);
+}
+
+// A*x accumulated in the accumulator precision: double products for the
+// reference's double accumulators, float products for the all-FP32 variant.
+template <typename AccT, typename T>
+__device__ __forceinline__ AccT acc_mul(T a, T x)
+{
+    if constexpr (sizeof(AccT) == 8)
+        return (double)a * (double)x;
+    else
+        return (float)(a * x);
+}
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+__global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
+                                              int warps_total)
+{
+    using G = Geom<CPL>;
+    if (ctl->active == 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+
+    StepK<T> k = rk.k;
+    k.dt = (T)ctl->dt;
+    k.den = (T)(2 * K) * k.dt;
+    k.rden = T(1) / k.den;
+    const T dt = k.dt, A = k.A;
+    const T F = (T)ctl->F;
+    const T tmax_val = (T)ctl->tmax_val;
+    const T inflow_dh = (T)ctl->inflow_dh;
+    const int want_v = ctl->want_v;
+    const T *hin = ctl->h_cur ? g.h1 : g.h0;
+    T *hout = ctl->h_cur ? g.h0 : g.h1;
+    const T rainv = rk.cr_uniform * F;   // C*Rday*F for a uniform field
+    const T dd = k.d_diag;
+    const T qnan = qnan_of<T>();
+
+    AccT a_rain = 0, a_clamp = 0, a_sea = 0, a_bnd = 0;
+    unsigned long long capn = 0;
+    T vmax = T(0);
+
+    const int nr = g.nr, nc = g.nc;
+    const int nstrips = (nc + G::OW - 1) / G::OW;
+    const long long total = (long long)nstrips * nr;
+    long long w0 = total * wid / warps_total, w1 = total * (wid + 1) / warps_total;
+    if (wid >= warps_total)
+        w0 = w1 = 0;
+
+    while (w0 < w1) {
+        const int strip = (int)(w0 / nr);
+        const int r0 = (int)(w0 % nr);
+        const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
+        w0 += r1 - r0;
+
+        const int cbase = strip * G::OW - G::HL + lane * CPL;   // first column of the lane
+        const bool out_lane = lane * CPL >= G::HL && lane * CPL < G::HL + G::OW;
+        const long long colo = (long long)(cbase + PADC);
+
+        // Pipeline registers; the comments give the rows they hold while
+        // iteration i runs stages C..E (face rows are the upper cell's row).
+        Row<T, CPL> nx, cu, p1, p2, p3;      // rows i+1, i, i-1, i-2, i-3
+        T X1[CPL], X2[CPL];                  // x-faces of rows i-1, i-2
+        T Y1[CPL], Y2[CPL];                  // y-faces of rows i-2, i-3
+        T E1[CPL], E2[CPL];                  // K=8 SE faces of rows i-2, i-3
+        T W1[CPL], W2[CPL];                  // K=8 SW faces of rows i-2, i-3
+        T s1[CPL], s2[CPL];                  // limiter of rows i-2, i-3
+        T qo1[CPL];                          // open-edge discharge of row i-2
+        int ko1[CPL];                        // open sides of row i-2
+        T L3[CPL], L4[CPL];                  // new level (NaN: WALL) of rows i-3, i-4
+        T hn3[CPL];                          // new depth of row i-3
+        T hm[CPL];                           // hmax of row i-2
+        T cr1[CPL];                          // rain field of row i-2
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            X1[j] = X2[j] = Y1[j] = Y2[j] = T(0);
+            E1[j] = E2[j] = W1[j] = W2[j] = T(0);
+            s1[j] = s2[j] = T(1);
+            qo1[j] = T(0);
+            ko1[j] = 0;
+            L3[j] = L4[j] = qnan;
+            hn3[j] = T(0);
+            hm[j] = T(0);
+            cr1[j] = T(0);
+            cu.z[j] = cu.h[j] = cu.n[j] = T(0);
+            cu.m[j] = M_WALL;
+        }
+        p1 = cu;
+        p2 = cu;
+        p3 = cu;
+        load_row<T, CPL>(nx, g, hin, (long long)(r0 - 3 + PADR) * g.pitch + colo);
+
+        for (int i = r0 - 3; i <= r1 + 2; i++) {
+            p3 = p2;
+            p2 = p1;
+            p1 = cu;
+            cu = nx;
+            load_row<T, CPL>(nx, g, hin, (long long)(i + 1 + PADR) * g.pitch + colo);
+            const bool row0_out = i >= r0 && i < r1;
+            const bool row1_out = i - 1 >= r0 && i - 1 < r1;
+            const bool row2_out = i - 2 >= r0 && i - 2 < r1;
+            // hmax and rain field of row i-1, used by stage D next iteration
+            const long long off1 = (long long)(i - 1 + PADR) * g.pitch + colo;
+            T hm_next[CPL], cr_next[CPL];
+            if (row1_out && out_lane)
+                VecIO<T, CPL>::ld_rw(hm_next, g.hmax + off1);
+            if constexpr (RAINF)
+                VecIO<T, CPL>::ld(cr_next, g.cr + off1);
+
+            // ---- A: x-faces of row i; y and diagonal faces of row i-1
+            T X0[CPL], Yn[CPL], En[CPL], Wn[CPL];
+            {
+                const T cz = sh_dn(cu.z[0]), ch = sh_dn(cu.h[0]), cn = sh_dn(cu.n[0]);
+                const uint32_t cm = sh_dn(cu.m[0]);
+                T pz = T(0), ph = T(0), pn = T(0);
+                uint32_t pm = M_WALL;
+                if constexpr (K == 8) {
+                    pz = sh_dn(p1.z[0]);
+                    ph = sh_dn(p1.h[0]);
+                    pn = sh_dn(p1.n[0]);
+                    pm = sh_dn(p1.m[0]);
+                }
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    int cap;
+                    const T zr = right_of<T, CPL>(cu.z, j, cz), hr = right_of<T, CPL>(cu.h, j, ch);
+                    const T nrr = right_of<T, CPL>(cu.n, j, cn);
+                    const uint32_t mr = right_of<uint32_t, CPL>(cu.m, j, cm);
+                    // x-face (i, c) -> (i, c+1)
+                    X0[j] = face_q<T, MATH>(cu.z[j], cu.h[j], cu.n[j], cu.m[j], zr, hr, nrr, mr,
+                                            k.dx, k.rdx, k, cap);
+                    if (row0_out && out_lane)
+                        capn += cap;
+                    // y-face (i-1, c) -> (i, c)
+                    Yn[j] = face_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], cu.z[j], cu.h[j],
+                                            cu.n[j], cu.m[j], k.dx, k.rdx, k, cap);
+                    if (row1_out && out_lane)
+                        capn += cap;
+                    if constexpr (K == 8) {
+                        // SE face (i-1, c) -> (i, c+1)
+                        En[j] = face_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], zr, hr, nrr, mr,
+                                                dd, k.rdd, k, cap);
+                        if (row1_out && out_lane)
+                            capn += cap;
+                        // SW face (i-1, c+1) -> (i, c)
+                        const T za = right_of<T, CPL>(p1.z, j, pz), ha = right_of<T, CPL>(p1.h, j, ph);
+                        const T na = right_of<T, CPL>(p1.n, j, pn);
+                        const uint32_t ma = right_of<uint32_t, CPL>(p1.m, j, pm);
+                        Wn[j] = face_q<T, MATH>(za, ha, na, ma, cu.z[j], cu.h[j], cu.n[j], cu.m[j],
+                                                dd, k.rdd, k, cap);
+                        if (row1_out && out_lane)
+                            capn += cap;
+                    } else {
+                        En[j] = Wn[j] = T(0);
+                    }
+                }
+            }
+
+            // ---- C: outflow and limiter of row i-1, in the reference face
+            //      order +x, -x, +y, -y, [d1+, d1-, d2+, d2-], open slots
+            T s0[CPL], qo0[CPL];
+            int ko0[CPL];
+            {
+                const T xl = sh_up(X1[CPL - 1]);
+                T el = T(0), wl = T(0);
+                if constexpr (K == 8) {
+                    el = sh_up(E1[CPL - 1]);
+                    wl = sh_up(Wn[CPL - 1]);
+                }
+                const int r = i - 1;
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    const int c = cbase + j;
+                    int kop = 0;
+                    if (rk.open && p1.m[j] == M_LAND)
+                        kop = (c == 0 && rk.edge_w) + (c == nc - 1 && rk.edge_e) +
+                              (r == 0 && rk.edge_n) + (r == nr - 1 && rk.edge_s);
+                    T qo = T(0);
+                    if (kop) {
+                        int cap;
+                        qo = open_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], k, cap);
+                        if (row1_out && out_lane)
+                            capn += (unsigned long long)(cap * kop);
+                    }
+                    qo0[j] = qo;
+                    ko0[j] = kop;
+                    T out = T(0), Q;
+                    Q = X1[j];
+                    if (Q > T(0)) out += Q;
+                    Q = left_of<T, CPL>(X1, j, xl);
+                    if (Q < T(0)) out += -Q;
+                    Q = Yn[j];
+                    if (Q > T(0)) out += Q;
+                    Q = Y1[j];
+                    if (Q < T(0)) out += -Q;
+                    if constexpr (K == 8) {
+                        Q = En[j];
+                        if (Q > T(0)) out += Q;
+                        Q = left_of<T, CPL>(E1, j, el);
+                        if (Q < T(0)) out += -Q;
+                        Q = left_of<T, CPL>(Wn, j, wl);
+                        if (Q > T(0)) out += Q;
+                        Q = W1[j];
+                        if (Q < T(0)) out += -Q;
+                    }
+                    out += open_sum<T>(qo, kop);
+                    const T ov = out * dt;
+                    s0[j] = p1.m[j] == M_LAND ? limiter_s<T, MATH>(ov, p1.h[j], A) : T(1);
+                }
+            }
+
+            // ---- D: limiter-scaled net inflow and depth update of row i-2
+            //      (s0: row i-1 below, s1: the row itself, s2: row i-3 above)
+            T hn2[CPL], Ln2[CPL];
+            {
+                const int r = i - 2;
+                const T sl = sh_up(s1[CPL - 1]), sr = sh_dn(s1[0]);
+                const T xl = sh_up(X2[CPL - 1]);
+                T bl = T(1), br = T(1), al = T(1), ar = T(1), el = T(0), wl = T(0);
+                if constexpr (K == 8) {
+                    bl = sh_up(s0[CPL - 1]);
+                    br = sh_dn(s0[0]);
+                    al = sh_up(s2[CPL - 1]);
+                    ar = sh_dn(s2[0]);
+                    el = sh_up(E2[CPL - 1]);
+                    wl = sh_up(W1[CPL - 1]);
+                }
+                uint32_t ml = 0, mr = 0, m1l = 0, m1r = 0, m3l = 0, m3r = 0;
+                if (rk.has_sea) {
+                    ml = sh_up(p2.m[CPL - 1]);
+                    mr = sh_dn(p2.m[0]);
+                    if constexpr (K == 8) {
+                        m1l = sh_up(p1.m[CPL - 1]);
+                        m1r = sh_dn(p1.m[0]);
+                        m3l = sh_up(p3.m[CPL - 1]);
+                        m3r = sh_dn(p3.m[0]);
+                    }
+                }
+                const bool sea_on = rk.has_sea != 0;
+                bool rose_any = false;
+                T hmx[CPL];
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    const uint32_t ma = p2.m[j];
+                    const bool land = ma == M_LAND;
+                    const T sa = s1[j];
+                    T net = T(0), Q, Qs;
+                    double sea = 0.0;
+                    // +x: face (r, c) -> (r, c+1)
+                    Q = X2[j];
+                    Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s1, j, sr));
+                    net -= Qs;
+                    if (sea_on && land && right_of<uint32_t, CPL>(p2.m, j, mr) == M_SEA && Qs > T(0))
+                        sea += (double)dt * (double)Qs;
+                    // -x: face (r, c-1) -> (r, c)
+                    Q = left_of<T, CPL>(X2, j, xl);
+                    Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s1, j, sl) : sa);
+                    net += Qs;
+                    if (sea_on && land && left_of<uint32_t, CPL>(p2.m, j, ml) == M_SEA && Qs < T(0))
+                        sea += (double)dt * (double)(-Qs);
+                    // +y: face (r, c) -> (r+1, c)
+                    Q = Y1[j];
+                    Qs = Q * (Q >= T(0) ? sa : s0[j]);
+                    net -= Qs;
+                    if (sea_on && land && p1.m[j] == M_SEA && Qs > T(0))
+                        sea += (double)dt * (double)Qs;
+                    // -y: face (r-1, c) -> (r, c)
+                    Q = Y2[j];
+                    Qs = Q * (Q >= T(0) ? s2[j] : sa);
+                    net += Qs;
+                    if (sea_on && land && p3.m[j] == M_SEA && Qs < T(0))
+                        sea += (double)dt * (double)(-Qs);
+                    if constexpr (K == 8) {
+                        // d1+: (r, c) -> (r+1, c+1)
+                        Q = E1[j];
+                        Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s0, j, br));
+                        net -= Qs;
+                        if (sea_on && land && right_of<uint32_t, CPL>(p1.m, j, m1r) == M_SEA &&
+                            Qs > T(0))
+                            sea += (double)dt * (double)Qs;
+                        // d1-: (r-1, c-1) -> (r, c)
+                        Q = left_of<T, CPL>(E2, j, el);
+                        Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s2, j, al) : sa);
+                        net += Qs;
+                        if (sea_on && land && left_of<uint32_t, CPL>(p3.m, j, m3l) == M_SEA &&
+                            Qs < T(0))
+                            sea += (double)dt * (double)(-Qs);
+                        // d2+: (r, c) -> (r+1, c-1), SW face of index (r, c-1)
+                        Q = left_of<T, CPL>(W1, j, wl);
+                        Qs = Q * (Q >= T(0) ? sa : left_of<T, CPL>(s0, j, bl));
+                        net -= Qs;
+                        if (sea_on && land && left_of<uint32_t, CPL>(p1.m, j, m1l) == M_SEA &&
+                            Qs > T(0))
+                            sea += (double)dt * (double)Qs;
+                        // d2-: (r-1, c+1) -> (r, c), SW face of index (r-1, c)
+                        Q = W2[j];
+                        Qs = Q * (Q >= T(0) ? right_of<T, CPL>(s2, j, ar) : sa);
+                        net += Qs;
+                        if (sea_on && land && right_of<uint32_t, CPL>(p3.m, j, m3r) == M_SEA &&
+                            Qs < T(0))
+                            sea += (double)dt * (double)(-Qs);
+                    }
+                    const T Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
+                    net -= Qo;
+                    T ha = p2.h[j];
+                    const bool cell_out = row2_out && out_lane;
+                    if (land) {
+                        const T rain = RAINF ? cr1[j] * F : rainv;
+                        ha = ha + (dt * Mth<T, MATH>::div(net, A) + rain);
+                        if (cell_out)
+                            a_rain += acc_mul<AccT, T>(A, rain);
+                        if (ha < T(0)) {
+                            if (cell_out)
+                                a_clamp += acc_mul<AccT, T>(-ha, A);
+                            ha = T(0);
+                        }
+                        if (r == rk.inflow_r && cbase + j == rk.inflow_c)
+                            ha = ha + inflow_dh;
+                    }
+                    if (cell_out) {
+                        a_sea += (AccT)sea;
+                        a_bnd += acc_mul<AccT, T>(dt, Qo);
+                    }
+                    hn2[j] = ha;
+                    Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
+                    hmx[j] = hm[j];
+                    if (cell_out && land && ha > hm[j]) {
+                        hmx[j] = ha;
+                        rose_any = true;
+                        g.tmax[(long long)(r + PADR) * g.pitch + colo + j] = tmax_val;
+                    }
+                }
+                if (row2_out && out_lane) {
+                    const long long off2 = (long long)(r + PADR) * g.pitch + colo;
+                    VecIO<T, CPL>::st(hout + off2, hn2);
+                    if (rose_any)
+                        VecIO<T, CPL>::st(g.hmax + off2, hmx);
+                }
+            }
+
+            // ---- E: next step's stable velocity of row i-3 from the new
+            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2)
+            if (want_v) {
+                const int r = i - 3;
+                const T Ll = sh_up(L3[CPL - 1]), Lr = sh_dn(L3[0]);
+                T L2l = T(0), L2r = T(0), L4l = T(0), L4r = T(0);
+                if constexpr (K == 8) {
+                    L2l = sh_up(Ln2[CPL - 1]);
+                    L2r = sh_dn(Ln2[0]);
+                    L4l = sh_up(L4[CPL - 1]);
+                    L4r = sh_dn(L4[0]);
+                }
+                if (r >= r0 && r < r1 && out_lane) {
+#pragma unroll
+                    for (int j = 0; j < CPL; j++) {
+                        const T hv = hn3[j];
+                        if (p3.m[j] != M_LAND || !(hv >= k.tau_h))
+                            continue;
+                        if (vmax > T(0) && Mth<T, MATH>::vcr_le(vmax, k.g, hv))
+                            continue;       // this cell cannot raise the maximum
+                        const int c = cbase + j;
+                        const T la = L3[j];
+                        T mo = T(0);
+                        mo = fmax(mo, fabs(la - right_of<T, CPL>(L3, j, Lr)));
+                        mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
+                        mo = fmax(mo, fabs(la - Ln2[j]));
+                        mo = fmax(mo, fabs(la - L4[j]));
+                        if (rk.open && ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e) ||
+                                        (r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s))) {
+                            const T lv = p3.z[j] - k.S_bnd * k.dx;
+                            mo = fmax(mo, fabs(la - lv));
+                        }
+                        T Smax = Mth<T, MATH>::div(mo, k.dx);
+                        if constexpr (K == 8) {
+                            T md = T(0);
+                            md = fmax(md, fabs(la - right_of<T, CPL>(Ln2, j, L2r)));
+                            md = fmax(md, fabs(la - left_of<T, CPL>(Ln2, j, L2l)));
+                            md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
+                            md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
+                            const T Sd = Mth<T, MATH>::div(md, dd);
+                            if (Sd > Smax)
+                                Smax = Sd;
+                        }
+                        const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
+                        if (v > vmax)
+                            vmax = v;
+                    }
+                }
+            }
+
+            // ---- advance the pipeline
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                X2[j] = X1[j];
+                X1[j] = X0[j];
+                Y2[j] = Y1[j];
+                Y1[j] = Yn[j];
+                if constexpr (K == 8) {
+                    E2[j] = E1[j];
+                    E1[j] = En[j];
+                    W2[j] = W1[j];
+                    W1[j] = Wn[j];
+                }
+                s2[j] = s1[j];
+                s1[j] = s0[j];
+                qo1[j] = qo0[j];
+                ko1[j] = ko0[j];
+                L4[j] = L3[j];
+                L3[j] = Ln2[j];
+                hn3[j] = hn2[j];
+                if (row1_out && out_lane)
+                    hm[j] = hm_next[j];
+                if constexpr (RAINF)
+                    cr1[j] = cr_next[j];
+            }
+        }
+    }
+
+    // ---- publish the warp's accumulators and velocity maximum
+    a_rain = warp_sum(a_rain);
+    a_clamp = warp_sum(a_clamp);
+    a_sea = warp_sum(a_sea);
+    a_bnd = warp_sum(a_bnd);
+    capn = warp_sum(capn);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T vo = __shfl_xor_sync(0xffffffffu, vmax, o);
+        vmax = vo > vmax ? vo : vmax;
+    }
+    if (lane == 0) {
+        const int slot = wid & (NSLOT - 1);
+        if constexpr (sizeof(AccT) == 8) {
+            if (a_rain != 0) atomicAdd(&ctl->accd[0][slot], (double)a_rain);
+            if (a_clamp != 0) atomicAdd(&ctl->accd[1][slot], (double)a_clamp);
+            if (a_sea != 0) atomicAdd(&ctl->accd[2][slot], (double)a_sea);
+            if (a_bnd != 0) atomicAdd(&ctl->accd[3][slot], (double)a_bnd);
+        } else {
+            if (a_rain != 0) atomicAdd(&ctl->accf[0][slot], (float)a_rain);
+            if (a_clamp != 0) atomicAdd(&ctl->accf[1][slot], (float)a_clamp);
+            if (a_sea != 0) atomicAdd(&ctl->accf[2][slot], (float)a_sea);
+            if (a_bnd != 0) atomicAdd(&ctl->accf[3][slot], (float)a_bnd);
+        }
+        if (capn)
+            atomicAdd(&ctl->cap[slot], capn);
+        if (want_v && vmax > T(0)) {
+            if constexpr (sizeof(T) == 4)
+                atomicMax(&ctl->vmax_bits, (unsigned long long)__float_as_uint((float)vmax));
+            else
+                atomicMax(&ctl->vmax_bits, (unsigned long long)__double_as_longlong((double)vmax));
+        }
+    }
+    // ---- the last CTA to finish prepares the next step
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->ctas_done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->h_cur ^= 1;
+            ctl->launches += 1;
+            finalize<T>(ctl, tc, rk, true);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
+// Initial dt: max stable velocity over the initial depth (one thread per
+// cell, run once per run), then the first step's control.
+
+template <typename T, int K, int MATH>
+__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl)
+{
+    const StepK<T> k = rk.k;
+    const T *h = ctl->h_cur ? g.h1 : g.h0;
+    T vmax = T(0);
+    const long long N = (long long)g.nr * g.nc;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / g.nc), c = (int)(idx % g.nc);
+        const long long a = (long long)(r + PADR) * g.pitch + c + PADC;
+        if (g.m[a] != M_LAND || !(h[a] >= k.tau_h))
+            continue;
+        const T la = g.z[a] + h[a];
+        T mo = T(0), md = T(0);
+        const long long nb[8] = {a + 1, a - 1, a + g.pitch, a - g.pitch,
+                                 a + g.pitch + 1, a + g.pitch - 1, a - g.pitch + 1,
+                                 a - g.pitch - 1};
+#pragma unroll
+        for (int q = 0; q < (K == 8 ? 8 : 4); q++) {
+            const uint32_t mb = g.m[nb[q]];
+            if (mb == M_WALL)
+                continue;
+            const T lb = mb == M_SEA ? k.z_sea : g.z[nb[q]] + h[nb[q]];
+            const T d = fabs(la - lb);
+            if (q < 4)
+                mo = fmax(mo, d);
+            else
+                md = fmax(md, d);
+        }
+        if (rk.open && ((c == 0 && rk.edge_w) || (c == g.nc - 1 && rk.edge_e) ||
+                        (r == 0 && rk.edge_n) || (r == g.nr - 1 && rk.edge_s)))
+            mo = fmax(mo, fabs(la - (g.z[a] - k.S_bnd * k.dx)));
+        T Smax = Mth<T, MATH>::div(mo, k.dx);
+        if (K == 8) {
+            const T Sd = Mth<T, MATH>::div(md, k.d_diag);
+            if (Sd > Smax)
+                Smax = Sd;
+        }
+        const T v = cell_velocity<T, MATH>(h[a], g.n[a], Smax, k);
+        if (v > vmax)
+            vmax = v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T vo = __shfl_xor_sync(0xffffffffu, vmax, o);
+        vmax = vo > vmax ? vo : vmax;
+    }
+    if ((threadIdx.x & 31) == 0 && vmax > T(0)) {
+        if constexpr (sizeof(T) == 4)
+            atomicMax(&ctl->vmax_bits, (unsigned long long)__float_as_uint((float)vmax));
+        else
+            atomicMax(&ctl->vmax_bits, (unsigned long long)__double_as_longlong((double)vmax));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->ctas_done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            finalize<T>(ctl, tc, rk, false);
+        }
+    }
+}
+
+// LAND volume sum(h*A) in double (FloodCA src/common/grid.c:125-141).
+template <typename T>
+__global__ void k_volume(GridD<T> g, const Ctl *ctl, T A, double *out)
+{
+    const T *h = ctl->h_cur ? g.h1 : g.h0;
+    double v = 0.0;
+    const long long N = (long long)g.nr * g.nc;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < N;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / g.nc), c = (int)(idx % g.nc);
+        const long long a = (long long)(r + PADR) * g.pitch + c + PADC;
+        if (g.m[a] == M_LAND)
+            v += (double)h[a] * (double)A;
+    }
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0 && v != 0.0)
+        atomicAdd(out, v);
+}
+
+}  // namespace fcab

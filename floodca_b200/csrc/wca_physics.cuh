@@ -1,0 +1,194 @@
+// Device formulas of the WCA rule, re-derived from FloodCA
+// src/kernels/physics.h for the sm_100a kernels. The expression order of
+// every rounded operation follows the reference so that the float build
+// (MATH_EXACT) and the double build give the reference's values; MATH_FAST
+// replaces cbrt, sqrt and divisions with hardware approximations.
+#pragma once
+
+#include "wca_math.cuh"
+
+namespace fcab {
+
+enum : uint8_t { M_LAND = 0, M_SEA = 1, M_WALL = 2 };
+enum { MATH_EXACT = 0, MATH_FAST = 1 };
+
+// Per-step constants shared by every face of one step.
+template <typename T>
+struct StepK {
+    T dx, A, g, tau_h, tau_l, z_sea, S_bnd;
+    T w;          // face width: dx (K=4) or (sqrt2-1)dx (K=8), physics.h:37-43
+    T d_diag;     // sqrt2*dx, physics.h:45-48
+    T dt;         // this step's dt
+    T den;        // (2K)*dt, denominator of the volume cap
+    T rden;       // RN(1/den), used to skip the cap division when far from capping
+    T rdx, rdd;   // 1/dx, 1/d_diag (fast mode)
+    T alpha_dx;   // alpha*dx
+    T inv_A;      // 1/A (fast mode)
+};
+
+// --- hf^(2/3), sqrt and Manning velocity in each precision / mode ---------
+
+template <typename T, int MATH>
+struct Mth;
+
+template <>
+struct Mth<float, MATH_EXACT> {
+    static __device__ __forceinline__ float cbrt_sq(float x) { return cbrt_sq_rn(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return __fsqrt_rn(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
+    static __device__ __forceinline__ float min_vcr(float v, float g, float h)
+    {
+        return min_vcr_rn(v, g, h);
+    }
+    static __device__ __forceinline__ bool vcr_le(float vmax, float g, float h)
+    {
+        return vcr_at_most(vmax, g, h);
+    }
+};
+
+template <>
+struct Mth<float, MATH_FAST> {
+    static __device__ __forceinline__ float cbrt_sq(float x)
+    {
+        return ex2_approx(lg2_approx(x) * 0.666666687f);
+    }
+    static __device__ __forceinline__ float sqrt_(float x) { return x * rsqrt_approx(x); }
+    static __device__ __forceinline__ float div(float a, float b) { return a * rcp_approx(b); }
+    static __device__ __forceinline__ float rcp(float a) { return rcp_approx(a); }
+    static __device__ __forceinline__ float min_vcr(float v, float g, float h)
+    {
+        float p = g * h;
+        float vcr = p * rsqrt_approx(p);
+        return v > vcr ? vcr : v;
+    }
+    static __device__ __forceinline__ bool vcr_le(float vmax, float g, float h)
+    {
+        return g * h * 1.0001f <= vmax * vmax;
+    }
+};
+
+template <int MATH>
+struct Mth<double, MATH> {
+    static __device__ __forceinline__ double cbrt_sq(double x) { return cbrt(x * x); }
+    static __device__ __forceinline__ double sqrt_(double x) { return __dsqrt_rn(x); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
+    static __device__ __forceinline__ double min_vcr(double v, double g, double h)
+    {
+        double vcr = __dsqrt_rn(g * h);
+        return v > vcr ? vcr : v;
+    }
+    static __device__ __forceinline__ bool vcr_le(double vmax, double g, double h)
+    {
+        return __dsqrt_rn(g * h) <= vmax;
+    }
+};
+
+// --- face discharge (physics.h:51-125) -------------------------------------
+
+// Signed discharge a->b across a face of centre distance d (dx, or the
+// diagonal distance). rd = 1/d for the fast mode. cap is set when the volume
+// cap |dL|*A/(2K*dt) binds.
+template <typename T, int MATH>
+__device__ __forceinline__ T face_q(T za, T ha, T na, uint32_t ma, T zb, T hb, T nb, uint32_t mb,
+                                    T d, T rd, const StepK<T> &k, int &cap)
+{
+    using M = Mth<T, MATH>;
+    cap = 0;
+    if (ma == M_WALL || mb == M_WALL)
+        return T(0);
+    const bool sa = ma == M_SEA, sb = mb == M_SEA;
+    T zea = sa ? k.z_sea : za;
+    T zeb = sb ? k.z_sea : zb;
+    T la = zea + (sa ? T(0) : ha);
+    T lb = zeb + (sb ? T(0) : hb);
+    T dL = la - lb;
+    T adL = dL < T(0) ? -dL : dL;
+    if (adL < k.tau_l)
+        return T(0);
+    T hf = (la > lb ? la : lb) - (zea > zeb ? zea : zeb);
+    if (hf < k.tau_h)
+        return T(0);
+    if (dL > T(0) ? sa : sb)
+        return T(0);
+    T nf = sa ? nb : (sb ? na : T(0.5) * (na + nb));
+    if (nf < T(1e-12))
+        nf = T(1e-12);
+    T S = MATH == MATH_EXACT ? M::div(adL, d) : adL * rd;
+    T v = M::rcp(nf) * M::cbrt_sq(hf) * M::sqrt_(S);
+    v = M::min_vcr(v, k.g, hf);
+    T Qm = v * hf * k.w;
+    T num = adL * k.A;
+    // Cap test: skip the exact division when the estimate num*rden is clearly
+    // above Qm (relative error of the estimate is below 2^-22).
+    if (MATH == MATH_EXACT) {
+        if (!(num * k.rden > Qm * T(1.0000005))) {
+            T Qc = M::div(num, k.den);
+            if (Qc < Qm) {
+                cap = 1;
+                Qm = Qc;
+            }
+        }
+    } else {
+        T Qc = num * k.rden;
+        if (Qc < Qm) {
+            cap = 1;
+            Qm = Qc;
+        }
+    }
+    return dL > T(0) ? Qm : -Qm;
+}
+
+// Open-edge discharge to the virtual neighbour z - S_bnd*dx, h = 0, same n,
+// distance dx, clipped at zero (FloodCA src/common/model.c:166-177).
+template <typename T, int MATH>
+__device__ __forceinline__ T open_q(T z, T h, T n, uint32_t m, const StepK<T> &k, int &cap)
+{
+    T Q = face_q<T, MATH>(z, h, n, m, z - k.S_bnd * k.dx, T(0), n, M_LAND, k.dx, k.rdx, k, cap);
+    return Q < T(0) ? T(0) : Q;
+}
+
+// Sum of k copies of q in the order of the reference's four open slots
+// (model.c:235-236): the zero slots do not change the partial sums.
+template <typename T>
+__device__ __forceinline__ T open_sum(T q, int kcnt)
+{
+    T s = kcnt > 0 ? q : T(0);
+    if (kcnt > 1)
+        s = s + q;
+    if (kcnt > 2)
+        s = s + q;
+    if (kcnt > 3)
+        s = s + q;
+    return s;
+}
+
+// Limiter (physics.h:127-134).
+template <typename T, int MATH>
+__device__ __forceinline__ T limiter_s(T out_vol, T h, T A)
+{
+    T hold = h * A;
+    if (out_vol > hold && out_vol > T(0))
+        return Mth<T, MATH>::div(hold, out_vol);
+    return T(1);
+}
+
+// Velocity whose alpha*dx/v is the cell's stable step (physics.h:193-217),
+// for a wet LAND cell (h >= tau_h); Smax is the largest surface slope.
+template <typename T, int MATH>
+__device__ __forceinline__ T cell_velocity(T h, T n, T Smax, const StepK<T> &k)
+{
+    using M = Mth<T, MATH>;
+    if (n < T(1e-12))
+        n = T(1e-12);
+    if (Smax < T(0))
+        Smax = T(0);
+    T v = M::rcp(n) * M::cbrt_sq(h) * M::sqrt_(Smax);
+    v = M::min_vcr(v, k.g, h);
+    if (v < T(1e-6))
+        v = T(1e-6);
+    return v;
+}
+
+}  // namespace fcab

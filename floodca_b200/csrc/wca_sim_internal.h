@@ -1,0 +1,39 @@
+// Session state behind the opaque FcabSim handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "floodca_b200.h"
+#include "wca_dispatch.h"
+
+struct FcabSim {
+    FcabConfig cfg;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t esize = 4;            // element size of the state (4 or 8)
+    long long pitch = 0;         // elements per padded row
+    int rows_alloc = 0;
+    size_t nelem = 0;            // elements per padded field
+    void *z = nullptr, *n = nullptr, *cr = nullptr, *h0 = nullptr, *h1 = nullptr;
+    void *hmax = nullptr, *tmax = nullptr;
+    uint8_t *m = nullptr;
+    void *tmpC = nullptr, *tmpR = nullptr;   // padded staging copies of C and Rday
+    fcab::Ctl *ctl = nullptr;    // device control block
+    void *ctl_host = nullptr;    // pinned mirror
+    void *scratch = nullptr;     // 64 bytes of device scratch
+    fcab::RunK<float> rkf;
+    fcab::RunK<double> rkd;
+    fcab::TimeCfg tc;
+    bool rain_field = false;
+    int cpl = 2, grid = 1, warps_total = 4, occupancy = 1;
+    fcab::Launchers L;
+    bool have_variant = false, variant_dirty = true;
+    cudaGraphExec_t graph = nullptr;
+    long long launches = 0;
+    bool uploaded = false, inited = false;
+    int h_cur_host = 0;
+    int step0 = 0;
+    double V0 = 0.0;
+    long long land_cells = 0, open_faces = 0, faces_per_step = 0;
+};

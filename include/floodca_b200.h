@@ -1,0 +1,316 @@
+/*
+ * floodca_b200 -- B200-native (sm_100a) weighted cellular-automata flood step.
+ *
+ * Two C-ABI surfaces:
+ *
+ * 1. The drop-in: the entry points of FloodCA's CUDA backend
+ *    (src/cuda/cuda_backend.h:14-32) with the same names, argument meaning,
+ *    return codes and struct layouts (src/common/fca_types.h:34-159), so the
+ *    reference's unmodified src/cuda/main_cuda.c and
+ *    src/hybrid/main_ens_mpi_cuda.c link against this library in place of
+ *    src/cuda/kernels.cu. Build the caller and this library with the same
+ *    FCA_DOUBLE setting (libfloodca_b200.so: float `real`;
+ *    libfloodca_b200_f64.so: double `real`). The struct block below uses the
+ *    reference's include guard, so including both headers is harmless.
+ *
+ * 2. The extended API (fcab_*): device-resident sessions for callers that keep
+ *    the state on the GPU (benchmarks, ensembles, the surrogate pipeline).
+ *    Plain pointers and sizes; no `real`, so it is the same in both builds and
+ *    lives in libfloodca_b200_core.so.
+ */
+#ifndef FLOODCA_B200_H
+#define FLOODCA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+/* ------------------------------------------------------------------------ */
+/* Reference ABI types (layout-identical to FloodCA src/common/fca_types.h).  */
+/* ------------------------------------------------------------------------ */
+#ifndef FCA_TYPES_H
+#define FCA_TYPES_H
+
+#ifdef FCA_DOUBLE
+typedef double real;
+#else
+typedef float real;
+#endif
+
+enum { FCA_LAND = 0, FCA_SEA = 1, FCA_WALL = 2 };
+enum { FCA_BND_OPEN = 0, FCA_BND_CLOSED = 1 };
+enum { FCA_HYETO_TRIANGLE = 0, FCA_HYETO_UNIFORM = 1 };
+
+#define FCA_MAX_FORCE_DAYS 64
+#define FCA_DAY_S 86400.0
+
+/* Physical parameters (fca_types.h:34-49). */
+typedef struct FcaPhys {
+    real dx, A, g, alpha, tau_h, tau_l, z_sea, dt_max, dt_min, S_bnd, h_flood;
+    int U, K, boundary;
+} FcaPhys;
+
+/* Run configuration (fca_types.h:51-86). */
+typedef struct FcaRunCfg {
+    FcaPhys phys;
+    real T_sim, out_every;
+    int diag_every, progress_every, hyeto;
+    real D_h, phi, lambda;
+    int steps, no_output, neigh;
+    char config_path[512], grid_dir[512], scenario[128], scenario_file[512];
+    char warmstart[512], rain_file[512], out_dir[512], csv_path[512], exp_id[32];
+    int repeat, threads, ranks, gpus, block_x, block_y;
+    char halo_mode[16], reduce_impl[16], gpu_model[64], backend[32], forcing_csv[512];
+    int n_force_days;
+    char force_files[FCA_MAX_FORCE_DAYS][768];
+} FcaRunCfg;
+
+struct FcaGrid;
+
+/* Distributed-memory hooks (fca_types.h:91-98); ignored by this library. */
+typedef struct FcaComm {
+    void *ctx;
+    int rank;
+    void (*halo)(struct FcaGrid *g, real *arr, void *ctx);
+    real (*min_real)(real v, void *ctx);
+    double (*sum_double)(double v, void *ctx);
+    int (*load_rday)(struct FcaGrid *g, const char *path, void *ctx);
+} FcaComm;
+
+/* Row-major host grid (fca_types.h:100-126). */
+typedef struct FcaGrid {
+    int nrows, ncols;
+    int r0, r1, c0, c1;
+    int edge_n, edge_s, edge_w, edge_e;
+    FcaComm *comm;
+    real dx, x0, y0;
+    real *z, *h, *n, *C;
+    uint8_t *mask;
+    real *Rday, *hmax, *tmax, *s, *out, *Qx, *Qy, *Qd1, *Qd2, *Qopen;
+} FcaGrid;
+
+/* Run accumulators (fca_types.h:128-142). */
+typedef struct FcaAcc {
+    double V, V0, V_rain, V_sea, V_bnd, clamp_err;
+    long cap_active, cap_total, dt_min_hits;
+    double t;
+    int step;
+    real dt_base;
+    int force_day;
+} FcaAcc;
+
+/* Phase timers (fca_types.h:144-159). */
+typedef struct FcaTimers {
+    double wall_total, t_init, t_flux, t_limiter, t_update, t_dt, t_io;
+    double t_h2d, t_d2h, t_halo, t_allreduce, bytes_per_step;
+    long active_cells;
+} FcaTimers;
+
+#endif /* FCA_TYPES_H */
+
+#if defined(__GNUC__)
+#define FCAB_API __attribute__((visibility("default")))
+#else
+#define FCAB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in entry points (FloodCA src/cuda/cuda_backend.h:14-32).             */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces fca_cuda_run (src/cuda/kernels.cu:617-776). Runs the whole
+ * simulation on the current device and returns with g->h, g->hmax, g->tmax
+ * downloaded and acc/tm filled as the reference does. Differences: every edge
+ * flag g->edge_{n,s,w,e} is honoured (the reference CUDA path treats all four
+ * edges as open); a CUDA failure returns -2 instead of exit(1); a fixed-step
+ * run (cfg->steps > 0) whose step would have dt <= 0 stops instead of
+ * looping forever. Returns 0, -1 on a bad block shape (same check as the
+ * reference), -2 on a device error. */
+FCAB_API int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *tm);
+
+/* Replaces fca_cuda_device_name (src/cuda/kernels.cu:606-615). */
+FCAB_API void fca_cuda_device_name(char *name, size_t n);
+
+/* Replaces fca_cuda_select_device (src/cuda/kernels.cu:778-788): binds device
+ * local_rank % count and returns its index, or -1. */
+FCAB_API int fca_cuda_select_device(int local_rank);
+
+/* Ensemble session (src/cuda/kernels.cu:790-1043). Static fields stay on the
+ * device; each run uploads h, hmax, tmax and Rday, runs like fca_cuda_run and
+ * adds hmax >= thr[j] on LAND into uint16 counts kept on the device. */
+typedef struct FcaCudaEns FcaCudaEns;
+FCAB_API FcaCudaEns *fca_cuda_ens_open(const FcaGrid *g, FcaRunCfg *cfg, int nthr, const double *thr);
+FCAB_API int fca_cuda_ens_run(FcaCudaEns *e, FcaGrid *g, const FcaRunCfg *cfg, FcaAcc *acc,
+                     FcaTimers *tm, long *flooded, double *max_depth, void (*poll)(void *),
+                     void *pctx, int poll_every);
+FCAB_API int fca_cuda_ens_counts(FcaCudaEns *e, uint16_t *host);
+FCAB_API void fca_cuda_ens_close(FcaCudaEns *e);
+
+/* ------------------------------------------------------------------------ */
+/* Extended API (libfloodca_b200_core.so). No reference counterpart.          */
+/* ------------------------------------------------------------------------ */
+
+enum {
+    FCAB_PREC_F32 = 0,     /* FP32 stencil, FP64 volume and time (reference float build) */
+    FCAB_PREC_F32_ALL = 1, /* FP32 stencil, FP32 accumulators and simulated time */
+    FCAB_PREC_F64 = 2      /* FP64 everywhere (reference FCA_DOUBLE build) */
+};
+
+enum {
+    FCAB_MATH_EXACT = 0,   /* every float op rounded as in the reference parity build */
+    FCAB_MATH_FAST = 1     /* hardware approximations for cbrt/sqrt/divide */
+};
+
+typedef struct FcabConfig {
+    int nrows, ncols;
+    int precision;            /* FCAB_PREC_* */
+    int math;                 /* FCAB_MATH_* */
+    int K, U, boundary;       /* neighbours 4|8, dt reuse, FCA_BND_* */
+    int edge_n, edge_s, edge_w, edge_e; /* open-boundary edges when boundary is open */
+    int hyeto;                /* FCA_HYETO_* */
+    int max_steps;            /* > 0: fixed step count (reference `steps`) */
+    double dx, g, alpha, tau_h, tau_l, z_sea, dt_max, dt_min, S_bnd;
+    double T_sim, out_every, D_h, phi;
+    double rain_end;          /* > 0: no rain for steps starting at t >= rain_end (an event) */
+    long long inflow_cell;    /* row*ncols+col of a LAND cell, or -1 */
+    double inflow_peak;       /* triangular hydrograph: 0 at t=0, peak (m^3/s) at */
+    double inflow_t_peak;     /*   inflow_t_peak, 0 at inflow_t_end; added after  */
+    double inflow_t_end;      /*   the clamp, before hmax                         */
+    int cols_per_lane;        /* 0 = autotuned; else 1, 2 or 4 */
+    int seg_rows;             /* 0 = autotuned; rows per warp segment */
+} FcabConfig;
+
+typedef struct FcabStats {
+    double t, dt_base;
+    int step, done;
+    double V, V0, V_rain, V_sea, V_bnd, clamp_err, V_in;
+    long long cap_active, cap_total, dt_min_hits;
+    double E_mass;            /* |V+V_sea+V_bnd-V_rain-V_in-V0-clamp| / (V_rain+V_in+V0) */
+} FcabStats;
+
+/* Error codes returned by the fcab_* calls (fcab_last_error() has the text). */
+enum {
+    FCAB_OK = 0,
+    FCAB_ERR_ARG = -1,     /* invalid argument or unsupported combination */
+    FCAB_ERR_CUDA = -2,    /* a CUDA call failed */
+    FCAB_ERR_STATE = -3,   /* call out of order (e.g. advance before upload) */
+    FCAB_ERR_IO = -4       /* file read failed */
+};
+
+/* Snapshot of the device step control, for host loops. */
+typedef struct FcabPoll {
+    double t, dt_base;
+    int step, done, pause, force_day;
+} FcabPoll;
+
+/* Launch shape chosen for a session. */
+typedef struct FcabInfo {
+    int cols_per_lane, grid, warps, ctas_per_sm, rain_field;
+    long long land_cells, faces_per_step, pitch;
+} FcabInfo;
+
+typedef struct FcabSim FcabSim;
+
+/* Fills cfg with the reference defaults (src/common/config.c:8-45) for an
+ * nrows x ncols grid. */
+FCAB_API void fcab_config_defaults(FcabConfig *cfg, int nrows, int ncols);
+
+/* Creates a session on the current device. stream is a cudaStream_t (NULL:
+ * the session creates its own). Returns 0 or a negative code. */
+FCAB_API int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *stream);
+
+/* Uploads row-major host fields of nrows*ncols values (float, or double for
+ * FCAB_PREC_F64). n, C, Rday, hmax and tmax may be NULL: n = 0.03, C = Rday = 0,
+ * hmax = h, tmax = 0 (FloodCA src/common/grid.c:197-235). Resets time,
+ * step and accumulators; V0 is the LAND volume of h. */
+FCAB_API int fcab_sim_upload(FcabSim *s, const void *z, const void *h, const void *n, const void *C,
+                    const void *Rday, const uint8_t *mask, const void *hmax, const void *tmax);
+
+/* Same, from device pointers with the session's element type. */
+FCAB_API int fcab_sim_upload_device(FcabSim *s, const void *z, const void *h, const void *n,
+                           const void *C, const void *Rday, const uint8_t *mask,
+                           const void *hmax, const void *tmax);
+
+/* Replaces the rain field C*Rday (host arrays; either may be NULL = unchanged). */
+FCAB_API int fcab_sim_set_rain(FcabSim *s, const void *C, const void *Rday);
+
+/* Enqueues up to nsteps steps on the session stream without waiting. Steps
+ * after the end of the run (T_sim or max_steps) do nothing. */
+FCAB_API int fcab_sim_advance(FcabSim *s, int nsteps);
+
+/* Runs to the end of the run (T_sim or max_steps) and waits. */
+FCAB_API int fcab_sim_run(FcabSim *s);
+
+/* Sets the run clock (time, step count, held dt of the U-step reuse and the
+ * loaded forcing day, -1 for none), recomputes V0 and the first step's dt.
+ * fcab_sim_upload calls it with zeros. */
+FCAB_API int fcab_sim_reset_time(FcabSim *s, double t, int step, double dt_base, int force_day);
+
+/* Waits for the queued steps and reads the device step control. */
+FCAB_API int fcab_sim_poll(FcabSim *s, FcabPoll *p);
+
+/* Clears a pause (forcing day changed, or a progress point), recording the
+ * forcing day now loaded. */
+FCAB_API int fcab_sim_resume(FcabSim *s, int force_day);
+
+/* Launch shape (strip width, grid) and grid statistics of the session. */
+FCAB_API int fcab_sim_info(FcabSim *s, FcabInfo *info);
+
+/* Changes the run parameters of a session (not its grid size, precision or
+ * K); takes effect at the next fcab_sim_reset_time. */
+FCAB_API int fcab_sim_set_config(FcabSim *s, const FcabConfig *cfg);
+
+/* Pause the run every nsteps steps (0: never) and whenever the forcing day
+ * index floor(t/86400) (clamped to n_force_days-1) differs from the loaded
+ * one (n_force_days 0: no forcing days). */
+FCAB_API int fcab_sim_set_pause_every(FcabSim *s, int nsteps, int n_force_days);
+
+/* Uploads the dynamic state only (h; hmax = h when NULL; tmax = 0 when NULL);
+ * the static fields stay resident. Call fcab_sim_reset_time afterwards. */
+FCAB_API int fcab_sim_upload_state(FcabSim *s, const void *h, const void *hmax, const void *tmax);
+
+/* Adds hmax >= thr[j] on LAND cells into the device array counts[j*N + a]
+ * (uint16, N = nrows*ncols, at most 4 thresholds) and returns the flooded
+ * cell counts and the largest LAND hmax (at least 0). */
+FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uint16_t *counts,
+                           long long *flooded, double *max_depth);
+
+/* The session's cudaStream_t. */
+FCAB_API void *fcab_sim_stream(FcabSim *s);
+
+/* Test hook: evaluates a device math helper on n host inputs (which = 0:
+ * RN(cbrt(x*x)) as the exact mode computes hf^(2/3); 1: min(x, RN(sqrt(g*y)));
+ * 2: the fast-mode hf^(2/3)) and writes n host outputs. */
+FCAB_API int fcab_math_probe(int which, const float *x, const float *y, float *out, long long n,
+                             float g);
+
+/* Waits, then fills st (computes the LAND volume V). */
+FCAB_API int fcab_sim_stats(FcabSim *s, FcabStats *st);
+
+/* Downloads h, hmax, tmax (any may be NULL) to host arrays. */
+FCAB_API int fcab_sim_download(FcabSim *s, void *h, void *hmax, void *tmax);
+
+/* Device pointers of the padded state, for zero-copy consumers: element
+ * (r, c) is at base + (r + pad_rows) * pitch + c + pad_cols. */
+FCAB_API int fcab_sim_layout(FcabSim *s, void **h, void **hmax, void **tmax, long long *pitch,
+                    int *pad_rows, int *pad_cols);
+
+/* Number of kernels the session has launched so far. */
+FCAB_API long long fcab_sim_launches(FcabSim *s);
+
+FCAB_API void fcab_sim_destroy(FcabSim *s);
+
+/* Last error message of the calling thread ("" if none). */
+FCAB_API const char *fcab_last_error(void);
+
+/* Library build identification (e.g. "floodca_b200 sm_100a"). */
+FCAB_API const char *fcab_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLOODCA_B200_H */

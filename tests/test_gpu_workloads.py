@@ -1,0 +1,70 @@
+"""The benchmark workloads on the GPU against the oracle at sizes the oracle
+finishes in seconds, and size-independent properties at full size."""
+import numpy as np
+import pytest
+
+from floodca_b200 import synth
+from floodca_b200.sim import run_session
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _diff(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max())
+
+
+@pytest.mark.parametrize("kind", ["f32", "f64"])
+def test_config1_full_size_matches_oracle(kind):
+    d, p = synth.config1()
+    r = run_session(d, p, precision=kind)
+    o = pyoracle.run(d, p, double=(kind == "f64"))
+    assert r["step"] == o["step"]
+    assert _diff(r["h"], o["h"]) <= 1e-6 and _diff(r["hmax"], o["hmax"]) <= 1e-6
+    assert abs(r["V"] - o["V"]) / o["V"] < 1e-9
+
+
+def test_config2_shape_with_inflow_matches_oracle():
+    d, p = synth.config2(n=512)
+    p = p.with_(T_sim=3 * 3600.0)
+    r = run_session(d, p, precision="f32")
+    o = pyoracle.run(d, p)
+    assert r["step"] == o["step"]
+    assert _diff(r["hmax"], o["hmax"]) <= 1e-6
+    assert r["V_in"] == pytest.approx(o["V_in"], rel=1e-12)
+    assert abs(r["V"] - o["V"]) / o["V"] < 1e-9
+
+
+def test_config3_shape_precision_variants():
+    d, p = synth.config3(n=256)
+    p = p.with_(T_sim=2 * 3600.0)
+    r32 = run_session(d, p, precision="f32")
+    r64 = run_session(d, p, precision="f64")
+    rall = run_session(d, p, precision="f32all")
+    o = pyoracle.run(d, p)
+    assert _diff(r32["hmax"], o["hmax"]) <= 1e-6
+    # FP32 against FP64: within the 1 mm bar on this case, mass balance tight
+    assert _diff(r32["hmax"], r64["hmax"]) < 1e-3
+    assert r32["E_mass"] < 1e-6 and r64["E_mass"] < 1e-12
+    assert _diff(rall["hmax"], r64["hmax"]) < 1e-2
+
+
+def test_fast_math_within_tolerance():
+    d, p = synth.config1()
+    ex = run_session(d, p, precision="f32", math="exact")
+    fa = run_session(d, p, precision="f32", math="fast")
+    assert _diff(ex["hmax"], fa["hmax"]) <= 1e-3
+    assert abs(ex["V"] - fa["V"]) / ex["V"] <= 1e-5
+
+
+def test_config2_full_size_properties():
+    """4096^2 run for 30 simulated minutes: mass balance, non-negative
+    depth, hmax >= h, and the inflow volume matches its closed form."""
+    d, p = synth.config2()
+    p = p.with_(T_sim=1800.0)
+    r = run_session(d, p, precision="f32")
+    assert r["E_mass"] < 1e-5
+    assert (r["h"] >= 0).all() and (r["hmax"] >= r["h"]).all()
+    tp = 3 * 3600.0
+    want = 0.5 * 500.0 * (1800.0 / tp) * 1800.0
+    assert r["V_in"] == pytest.approx(want, rel=1e-9)

@@ -15,6 +15,7 @@ struct VariantKey {
     int cpl;    // 1, 2 or 4
     int math;   // MATH_*
     int rainf;  // per-cell rain field
+    int landonly; // every cell LAND (mask not read, padding at PAD_Z)
 };
 
 // Type-erased launchers; `g`, `rk` point at GridD<T>/RunK<T> of the variant's T.
@@ -31,11 +32,11 @@ bool lookup_f32(const VariantKey &k, Launchers *out);
 bool lookup_f32all(const VariantKey &k, Launchers *out);
 bool lookup_f64(const VariantKey &k, Launchers *out);
 
-template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LAND>
 cudaError_t launch_step(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
                         int warps_total, int grid, cudaStream_t s)
 {
-    k_step<T, AccT, K, CPL, MATH, RAINF><<<grid, 128, 0, s>>>(
+    k_step<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, 128, 0, s>>>(
         *static_cast<const GridD<T> *>(g), *static_cast<const RunK<T> *>(rk), tc, ctl,
         warps_total);
     return cudaGetLastError();
@@ -50,13 +51,13 @@ cudaError_t launch_init(const void *g, const void *rk, const TimeCfg &tc, Ctl *c
     return cudaGetLastError();
 }
 
-template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LAND>
 Launchers make_launchers()
 {
     Launchers L;
-    L.step = &launch_step<T, AccT, K, CPL, MATH, RAINF>;
+    L.step = &launch_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
     L.init = &launch_init<T, K, MATH>;
-    L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF>;
+    L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
     return L;
 }
 
@@ -66,7 +67,8 @@ bool lookup_kcr(const VariantKey &k, Launchers *out)
 {
 #define FCAB_CASE(KK, CC, RR)                                                    \
     if (k.K == KK && k.cpl == CC && (k.rainf != 0) == RR) {                      \
-        *out = make_launchers<T, AccT, KK, CC, MATH, RR>();                     \
+        *out = k.landonly ? make_launchers<T, AccT, KK, CC, MATH, RR, true>()   \
+                          : make_launchers<T, AccT, KK, CC, MATH, RR, false>(); \
         return true;                                                             \
     }
     FCAB_CASE(4, 1, false) FCAB_CASE(4, 1, true)

@@ -38,6 +38,7 @@ namespace fcab {
 constexpr int PADR = 4;   // padded rows above and below the grid
 constexpr int PADC = 4;   // padded columns left of the grid
 constexpr int NSLOT = 32; // accumulator slots (spread the atomics)
+constexpr double PAD_Z = 1e30;   // padding elevation of all-LAND grids
 
 template <int CPL>
 struct Geom {
@@ -366,14 +367,20 @@ struct Row {
     uint32_t m[CPL];
 };
 
-template <typename T, int CPL>
+template <typename T, int CPL, bool LANDONLY>
 __device__ __forceinline__ void load_row(Row<T, CPL> &R, const GridD<T> &g, const T *hin,
                                          long long off)
 {
     VecIO<T, CPL>::ld(R.z, g.z + off);
     VecIO<T, CPL>::ld(R.h, hin + off);
     VecIO<T, CPL>::ld(R.n, g.n + off);
-    ld_mask<CPL>(R.m, g.m + off);
+    if constexpr (LANDONLY) {
+#pragma unroll
+        for (int j = 0; j < CPL; j++)
+            R.m[j] = M_LAND;
+    } else {
+        ld_mask<CPL>(R.m, g.m + off);
+    }
 }
 
 template <typename T>
@@ -398,6 +405,23 @@ template <typename T, int CPL>
 __device__ __forceinline__ T left_of(const T (&x)[CPL], int j, T prv_last)
 {
     return j > 0 ? x[j > 0 ? j - 1 : 0] : prv_last;
+}
+
+// Maximum over the warp of a non-negative value (positive floats order like
+// their bit patterns, so the integer warp reduction applies).
+template <typename T>
+__device__ __forceinline__ T warp_max_nonneg(T v)
+{
+    if constexpr (sizeof(T) == 4) {
+        return __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(v)));
+    } else {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        return v;
+    }
 }
 
 template <typename A>
@@ -436,7 +460,10 @@ __device__ __forceinline__ AccT acc_mul(T a, T x)
         return (float)(a * x);
 }
 
-template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF>
+// LANDONLY: every cell of the grid is LAND; the mask is not read and the
+// padding around the grid carries z = PAD_Z (> any terrain), h = 0, which
+// makes every face to it carry zero discharge (hf = max(L) - max(z) = 0).
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
 __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
                                               int warps_total)
 {
@@ -462,7 +489,9 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
     const T qnan = qnan_of<T>();
 
     AccT a_rain = 0, a_clamp = 0, a_sea = 0, a_bnd = 0;
-    unsigned long long capn = 0;
+    double rain_sum = 0.0;       // sum of rain depths (per-cell rain field)
+    long long rain_cells = 0;    // LAND output cells (uniform rain)
+    unsigned capn = 0;
     T vmax = T(0);
 
     const int nr = g.nr, nc = g.nc;
@@ -481,6 +510,14 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
         const int cbase = strip * G::OW - G::HL + lane * CPL;   // first column of the lane
         const bool out_lane = lane * CPL >= G::HL && lane * CPL < G::HL + G::OW;
         const long long colo = (long long)(cbase + PADC);
+        // columns of this lane inside the grid (padding columns are WALL in the
+        // generic layout, but LAND-like in the LANDONLY layout)
+        bool colok[CPL];
+#pragma unroll
+        for (int j = 0; j < CPL; j++)
+            colok[j] = !LANDONLY || (cbase + j >= 0 && cbase + j < nc);
+        // does this lane hold column 0 or column nc-1 (open-edge candidates)?
+        const bool edge_lane = (cbase <= 0 && cbase + CPL > 0) || (cbase <= nc - 1 && cbase + CPL > nc - 1);
 
         // Pipeline registers; the comments give the rows they hold while
         // iteration i runs stages C..E (face rows are the upper cell's row).
@@ -513,14 +550,14 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
         p1 = cu;
         p2 = cu;
         p3 = cu;
-        load_row<T, CPL>(nx, g, hin, (long long)(r0 - 3 + PADR) * g.pitch + colo);
+        load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(r0 - 3 + PADR) * g.pitch + colo);
 
         for (int i = r0 - 3; i <= r1 + 2; i++) {
             p3 = p2;
             p2 = p1;
             p1 = cu;
             cu = nx;
-            load_row<T, CPL>(nx, g, hin, (long long)(i + 1 + PADR) * g.pitch + colo);
+            load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(i + 1 + PADR) * g.pitch + colo);
             const bool row0_out = i >= r0 && i < r1;
             const bool row1_out = i - 1 >= r0 && i - 1 < r1;
             const bool row2_out = i - 2 >= r0 && i - 2 < r1;
@@ -532,52 +569,79 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
             if constexpr (RAINF)
                 VecIO<T, CPL>::ld(cr_next, g.cr + off1);
 
-            // ---- A: x-faces of row i; y and diagonal faces of row i-1
+            // ---- A: x-faces of row i; y and diagonal faces of row i-1,
+            //      all evaluated together (faces_q) for instruction-level
+            //      parallelism across the NF independent faces
             T X0[CPL], Yn[CPL], En[CPL], Wn[CPL];
             {
+                constexpr int NF = (K == 8 ? 4 : 2) * CPL;
                 const T cz = sh_dn(cu.z[0]), ch = sh_dn(cu.h[0]), cn = sh_dn(cu.n[0]);
-                const uint32_t cm = sh_dn(cu.m[0]);
+                const uint32_t cm = LANDONLY ? (uint32_t)M_LAND : sh_dn(cu.m[0]);
                 T pz = T(0), ph = T(0), pn = T(0);
-                uint32_t pm = M_WALL;
+                uint32_t pm = M_LAND;
                 if constexpr (K == 8) {
                     pz = sh_dn(p1.z[0]);
                     ph = sh_dn(p1.h[0]);
                     pn = sh_dn(p1.n[0]);
-                    pm = sh_dn(p1.m[0]);
+                    if constexpr (!LANDONLY)
+                        pm = sh_dn(p1.m[0]);
                 }
+                T fza[NF], fha[NF], fna[NF], fzb[NF], fhb[NF], fnb[NF], fd[NF], frd[NF];
+                uint32_t fma_[NF], fmb[NF];
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
-                    int cap;
                     const T zr = right_of<T, CPL>(cu.z, j, cz), hr = right_of<T, CPL>(cu.h, j, ch);
                     const T nrr = right_of<T, CPL>(cu.n, j, cn);
                     const uint32_t mr = right_of<uint32_t, CPL>(cu.m, j, cm);
                     // x-face (i, c) -> (i, c+1)
-                    X0[j] = face_q<T, MATH>(cu.z[j], cu.h[j], cu.n[j], cu.m[j], zr, hr, nrr, mr,
-                                            k.dx, k.rdx, k, cap);
-                    if (row0_out && out_lane)
-                        capn += cap;
+                    fza[j] = cu.z[j]; fha[j] = cu.h[j]; fna[j] = cu.n[j]; fma_[j] = cu.m[j];
+                    fzb[j] = zr; fhb[j] = hr; fnb[j] = nrr; fmb[j] = mr;
+                    fd[j] = k.dx; frd[j] = k.rdx;
                     // y-face (i-1, c) -> (i, c)
-                    Yn[j] = face_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], cu.z[j], cu.h[j],
-                                            cu.n[j], cu.m[j], k.dx, k.rdx, k, cap);
-                    if (row1_out && out_lane)
-                        capn += cap;
+                    const int y = CPL + j;
+                    fza[y] = p1.z[j]; fha[y] = p1.h[j]; fna[y] = p1.n[j]; fma_[y] = p1.m[j];
+                    fzb[y] = cu.z[j]; fhb[y] = cu.h[j]; fnb[y] = cu.n[j]; fmb[y] = cu.m[j];
+                    fd[y] = k.dx; frd[y] = k.rdx;
                     if constexpr (K == 8) {
                         // SE face (i-1, c) -> (i, c+1)
-                        En[j] = face_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], zr, hr, nrr, mr,
-                                                dd, k.rdd, k, cap);
-                        if (row1_out && out_lane)
-                            capn += cap;
+                        const int e = 2 * CPL + j;
+                        fza[e] = p1.z[j]; fha[e] = p1.h[j]; fna[e] = p1.n[j]; fma_[e] = p1.m[j];
+                        fzb[e] = zr; fhb[e] = hr; fnb[e] = nrr; fmb[e] = mr;
+                        fd[e] = dd; frd[e] = k.rdd;
                         // SW face (i-1, c+1) -> (i, c)
-                        const T za = right_of<T, CPL>(p1.z, j, pz), ha = right_of<T, CPL>(p1.h, j, ph);
-                        const T na = right_of<T, CPL>(p1.n, j, pn);
-                        const uint32_t ma = right_of<uint32_t, CPL>(p1.m, j, pm);
-                        Wn[j] = face_q<T, MATH>(za, ha, na, ma, cu.z[j], cu.h[j], cu.n[j], cu.m[j],
-                                                dd, k.rdd, k, cap);
-                        if (row1_out && out_lane)
-                            capn += cap;
+                        const int w = 3 * CPL + j;
+                        fza[w] = right_of<T, CPL>(p1.z, j, pz);
+                        fha[w] = right_of<T, CPL>(p1.h, j, ph);
+                        fna[w] = right_of<T, CPL>(p1.n, j, pn);
+                        fma_[w] = right_of<uint32_t, CPL>(p1.m, j, pm);
+                        fzb[w] = cu.z[j]; fhb[w] = cu.h[j]; fnb[w] = cu.n[j]; fmb[w] = cu.m[j];
+                        fd[w] = dd; frd[w] = k.rdd;
+                    }
+                }
+                T fq[NF];
+                unsigned fc[NF];
+                faces_q<T, MATH, LANDONLY, NF>(fza, fha, fna, fma_, fzb, fhb, fnb, fmb, fd, frd, k,
+                                               fq, fc);
+                unsigned c0 = 0u, c1 = 0u;
+#pragma unroll
+                for (int j = 0; j < CPL; j++) {
+                    X0[j] = fq[j];
+                    Yn[j] = fq[CPL + j];
+                    c0 += fc[j];
+                    c1 += fc[CPL + j];
+                    if constexpr (K == 8) {
+                        En[j] = fq[2 * CPL + j];
+                        Wn[j] = fq[3 * CPL + j];
+                        c1 += fc[2 * CPL + j] + fc[3 * CPL + j];
                     } else {
                         En[j] = Wn[j] = T(0);
                     }
+                }
+                if (out_lane) {
+                    if (row0_out)
+                        capn += c0;
+                    if (row1_out)
+                        capn += c1;
                 }
             }
 
@@ -593,11 +657,12 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                     wl = sh_up(Wn[CPL - 1]);
                 }
                 const int r = i - 1;
+                const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
                     const int c = cbase + j;
                     int kop = 0;
-                    if (rk.open && p1.m[j] == M_LAND)
+                    if ((edge_row || edge_lane) && rk.open && p1.m[j] == M_LAND)
                         kop = (c == 0 && rk.edge_w) + (c == nc - 1 && rk.edge_e) +
                               (r == 0 && rk.edge_n) + (r == nr - 1 && rk.edge_s);
                     T qo = T(0);
@@ -605,32 +670,26 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                         int cap;
                         qo = open_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], k, cap);
                         if (row1_out && out_lane)
-                            capn += (unsigned long long)(cap * kop);
+                            capn += (unsigned)(cap * kop);
                     }
                     qo0[j] = qo;
                     ko0[j] = kop;
-                    T out = T(0), Q;
-                    Q = X1[j];
-                    if (Q > T(0)) out += Q;
-                    Q = left_of<T, CPL>(X1, j, xl);
-                    if (Q < T(0)) out += -Q;
-                    Q = Yn[j];
-                    if (Q > T(0)) out += Q;
-                    Q = Y1[j];
-                    if (Q < T(0)) out += -Q;
+                    // positive outgoing parts in the reference order; adding a
+                    // zero leaves a non-negative sum unchanged
+                    T out = T(0);
+                    out += fmax(X1[j], T(0));
+                    out += fmax(-left_of<T, CPL>(X1, j, xl), T(0));
+                    out += fmax(Yn[j], T(0));
+                    out += fmax(-Y1[j], T(0));
                     if constexpr (K == 8) {
-                        Q = En[j];
-                        if (Q > T(0)) out += Q;
-                        Q = left_of<T, CPL>(E1, j, el);
-                        if (Q < T(0)) out += -Q;
-                        Q = left_of<T, CPL>(Wn, j, wl);
-                        if (Q > T(0)) out += Q;
-                        Q = W1[j];
-                        if (Q < T(0)) out += -Q;
+                        out += fmax(En[j], T(0));
+                        out += fmax(-left_of<T, CPL>(E1, j, el), T(0));
+                        out += fmax(left_of<T, CPL>(Wn, j, wl), T(0));
+                        out += fmax(-W1[j], T(0));
                     }
                     out += open_sum<T>(qo, kop);
                     const T ov = out * dt;
-                    s0[j] = p1.m[j] == M_LAND ? limiter_s<T, MATH>(ov, p1.h[j], A) : T(1);
+                    s0[j] = p1.m[j] == M_LAND ? limiter_bf<T, MATH>(ov, p1.h[j], A) : T(1);
                 }
             }
 
@@ -662,6 +721,8 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                     }
                 }
                 const bool sea_on = rk.has_sea != 0;
+                const bool inflow_row = r == rk.inflow_r;
+                T *tm_row = g.tmax + (long long)(r + PADR) * g.pitch + colo;
                 bool rose_any = false;
                 T hmx[CPL];
 #pragma unroll
@@ -728,31 +789,47 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                     const T Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
                     net -= Qo;
                     T ha = p2.h[j];
-                    const bool cell_out = row2_out && out_lane;
+                    const bool cell_out = row2_out && out_lane && colok[j];
                     if (land) {
                         const T rain = RAINF ? cr1[j] * F : rainv;
-                        ha = ha + (dt * Mth<T, MATH>::div(net, A) + rain);
-                        if (cell_out)
-                            a_rain += acc_mul<AccT, T>(A, rain);
+                        ha = ha + (dt * Mth<T, MATH>::div_c(net, A, k.inv_A) + rain);
+                        if (cell_out) {
+                            // sum(A*rain) = A*sum(rain): A*rain is exact in double
+                            if constexpr (sizeof(AccT) == 4)
+                                a_rain += A * rain;
+                            else if constexpr (RAINF)
+                                rain_sum += (double)rain;
+                            else
+                                rain_cells += 1;
+                        }
                         if (ha < T(0)) {
                             if (cell_out)
                                 a_clamp += acc_mul<AccT, T>(-ha, A);
                             ha = T(0);
                         }
-                        if (r == rk.inflow_r && cbase + j == rk.inflow_c)
+                        if (inflow_row && cbase + j == rk.inflow_c)
                             ha = ha + inflow_dh;
                     }
                     if (cell_out) {
-                        a_sea += (AccT)sea;
-                        a_bnd += acc_mul<AccT, T>(dt, Qo);
+                        if (sea_on)
+                            a_sea += (AccT)sea;
+                        if (ko1[j])
+                            a_bnd += acc_mul<AccT, T>(dt, Qo);
                     }
-                    hn2[j] = ha;
-                    Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
+                    if constexpr (LANDONLY) {
+                        // outside the grid: keep the padding depth, no face
+                        const bool inside = colok[j] && p2.z[j] < T(0.5 * PAD_Z);
+                        hn2[j] = inside ? ha : p2.h[j];
+                        Ln2[j] = inside ? p2.z[j] + ha : qnan;
+                    } else {
+                        hn2[j] = ha;
+                        Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
+                    }
                     hmx[j] = hm[j];
                     if (cell_out && land && ha > hm[j]) {
                         hmx[j] = ha;
                         rose_any = true;
-                        g.tmax[(long long)(r + PADR) * g.pitch + colo + j] = tmax_val;
+                        tm_row[j] = tmax_val;
                     }
                 }
                 if (row2_out && out_lane) {
@@ -764,9 +841,12 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
             }
 
             // ---- E: next step's stable velocity of row i-3 from the new
-            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2)
+            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2). Cells whose
+            //      critical velocity cannot exceed the warp's running maximum
+            //      are skipped (their velocity is capped by it).
             if (want_v) {
                 const int r = i - 3;
+                const T thr = warp_max_nonneg(vmax);
                 const T Ll = sh_up(L3[CPL - 1]), Lr = sh_dn(L3[0]);
                 T L2l = T(0), L2r = T(0), L4l = T(0), L4r = T(0);
                 if constexpr (K == 8) {
@@ -775,14 +855,15 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                     L4l = sh_up(L4[CPL - 1]);
                     L4r = sh_dn(L4[0]);
                 }
+                const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
                 if (r >= r0 && r < r1 && out_lane) {
 #pragma unroll
                     for (int j = 0; j < CPL; j++) {
                         const T hv = hn3[j];
-                        if (p3.m[j] != M_LAND || !(hv >= k.tau_h))
+                        if (p3.m[j] != M_LAND || !colok[j] || !(hv >= k.tau_h))
                             continue;
-                        if (vmax > T(0) && Mth<T, MATH>::vcr_le(vmax, k.g, hv))
-                            continue;       // this cell cannot raise the maximum
+                        if (thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, hv))
+                            continue;
                         const int c = cbase + j;
                         const T la = L3[j];
                         T mo = T(0);
@@ -790,8 +871,8 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                         mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
                         mo = fmax(mo, fabs(la - Ln2[j]));
                         mo = fmax(mo, fabs(la - L4[j]));
-                        if (rk.open && ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e) ||
-                                        (r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s))) {
+                        if (edge_row || (edge_lane && rk.open &&
+                                         ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e)))) {
                             const T lv = p3.z[j] - k.S_bnd * k.dx;
                             mo = fmax(mo, fabs(la - lv));
                         }
@@ -842,6 +923,12 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
     }
 
     // ---- publish the warp's accumulators and velocity maximum
+    if constexpr (sizeof(AccT) == 8) {
+        if constexpr (RAINF)
+            a_rain = (double)A * rain_sum;
+        else
+            a_rain = (double)rain_cells * ((double)A * (double)rainv);
+    }
     a_rain = warp_sum(a_rain);
     a_clamp = warp_sum(a_clamp);
     a_sea = warp_sum(a_sea);
@@ -866,7 +953,7 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
             if (a_bnd != 0) atomicAdd(&ctl->accf[3][slot], (float)a_bnd);
         }
         if (capn)
-            atomicAdd(&ctl->cap[slot], capn);
+            atomicAdd(&ctl->cap[slot], (unsigned long long)capn);
         if (want_v && vmax > T(0)) {
             if constexpr (sizeof(T) == 4)
                 atomicMax(&ctl->vmax_bits, (unsigned long long)__float_as_uint((float)vmax));

@@ -33,6 +33,23 @@ struct Mth;
 
 template <>
 struct Mth<float, MATH_EXACT> {
+    // a/b given rb = RN(1/b): Markstein's correction, exact for normal operands
+    static __device__ __forceinline__ float div_c(float a, float b, float rb)
+    {
+        return div_mk(a, b, rb);
+    }
+    static __device__ __forceinline__ float rcp_bf(float a) { return rcp_nr(a); }
+    static __device__ __forceinline__ float sqrt_bf(float a) { return sqrt_nr(a); }
+    static __device__ __forceinline__ bool cbrt_try(float x, float &y, float &e)
+    {
+        return cbrt_sq_try(x, y, e);
+    }
+    static __device__ __forceinline__ float cbrt_settle(float x, float y, float e)
+    {
+        return cbrt_sq_settle(x, y, e);
+    }
+    static __device__ __forceinline__ bool caps(float v, float g, float h) { return vcr_caps(v, g, h); }
+    static __device__ __forceinline__ float vcr(float g, float h) { return sqrt_prod_rn(g, h); }
     static __device__ __forceinline__ float cbrt_sq(float x) { return cbrt_sq_rn(x); }
     static __device__ __forceinline__ float sqrt_(float x) { return __fsqrt_rn(x); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
@@ -49,6 +66,22 @@ struct Mth<float, MATH_EXACT> {
 
 template <>
 struct Mth<float, MATH_FAST> {
+    static __device__ __forceinline__ float div_c(float a, float, float rb) { return a * rb; }
+    static __device__ __forceinline__ float rcp_bf(float a) { return rcp_approx(a); }
+    static __device__ __forceinline__ float sqrt_bf(float a) { return a * rsqrt_approx(a); }
+    static __device__ __forceinline__ bool cbrt_try(float x, float &y, float &e)
+    {
+        y = ex2_approx(lg2_approx(x) * 0.666666687f);
+        e = 0.0f;
+        return false;
+    }
+    static __device__ __forceinline__ float cbrt_settle(float, float y, float) { return y; }
+    static __device__ __forceinline__ bool caps(float v, float g, float h) { return v * v > g * h; }
+    static __device__ __forceinline__ float vcr(float g, float h)
+    {
+        const float p = g * h;
+        return p * rsqrt_approx(p);
+    }
     static __device__ __forceinline__ float cbrt_sq(float x)
     {
         return ex2_approx(lg2_approx(x) * 0.666666687f);
@@ -70,6 +103,24 @@ struct Mth<float, MATH_FAST> {
 
 template <int MATH>
 struct Mth<double, MATH> {
+    static __device__ __forceinline__ double div_c(double a, double b, double)
+    {
+        return __ddiv_rn(a, b);
+    }
+    static __device__ __forceinline__ double rcp_bf(double a) { return __drcp_rn(a); }
+    static __device__ __forceinline__ double sqrt_bf(double a) { return __dsqrt_rn(a); }
+    static __device__ __forceinline__ bool cbrt_try(double x, double &y, double &e)
+    {
+        y = cbrt(x * x);
+        e = 0.0;
+        return false;
+    }
+    static __device__ __forceinline__ double cbrt_settle(double, double y, double) { return y; }
+    static __device__ __forceinline__ bool caps(double v, double g, double h)
+    {
+        return v > __dsqrt_rn(g * h);
+    }
+    static __device__ __forceinline__ double vcr(double g, double h) { return __dsqrt_rn(g * h); }
     static __device__ __forceinline__ double cbrt_sq(double x) { return cbrt(x * x); }
     static __device__ __forceinline__ double sqrt_(double x) { return __dsqrt_rn(x); }
     static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
@@ -138,6 +189,102 @@ __device__ __forceinline__ T face_q(T za, T ha, T na, uint32_t ma, T zb, T hb, T
         }
     }
     return dL > T(0) ? Qm : -Qm;
+}
+
+// Discharge of NF independent faces at once (the same formula as face_q),
+// arranged in phases so that each phase is one branch-free block over all
+// faces: the compiler interleaves the faces' dependency chains. Faces that
+// carry no flow (walls, |dL| < tau_l, hf < tau_h, upwind SEA) are evaluated
+// on safe operands and zeroed at the end. The rare exact-rounding
+// settlements (cube root near a midpoint, critical-velocity cap) run after
+// their phase in per-lane blocks.
+template <typename T, int MATH, bool LANDONLY, int NF>
+__device__ __forceinline__ void faces_q(const T (&za)[NF], const T (&ha)[NF], const T (&na)[NF],
+                                        const uint32_t (&ma)[NF], const T (&zb)[NF],
+                                        const T (&hb)[NF], const T (&nb)[NF],
+                                        const uint32_t (&mb)[NF], const T (&d)[NF],
+                                        const T (&rd)[NF], const StepK<T> &k, T (&Q)[NF],
+                                        unsigned (&cap)[NF])
+{
+    using M = Mth<T, MATH>;
+    T hf[NF], aL[NF], nf[NF], cb[NF], ce[NF];
+    bool dead[NF], pos[NF];
+    unsigned settle = 0u;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        T zea, zeb, la, lb, n;
+        bool dd = false;
+        if constexpr (LANDONLY) {
+            zea = za[f];
+            zeb = zb[f];
+            la = za[f] + ha[f];
+            lb = zb[f] + hb[f];
+            n = T(0.5) * (na[f] + nb[f]);
+        } else {
+            const bool sa = ma[f] == M_SEA, sb = mb[f] == M_SEA;
+            dd = ma[f] == M_WALL || mb[f] == M_WALL;
+            zea = sa ? k.z_sea : za[f];
+            zeb = sb ? k.z_sea : zb[f];
+            la = zea + (sa ? T(0) : ha[f]);
+            lb = zeb + (sb ? T(0) : hb[f]);
+            n = sa ? nb[f] : (sb ? na[f] : T(0.5) * (na[f] + nb[f]));
+            dd = dd || ((la - lb) > T(0) ? sa : sb);
+        }
+        const T dL = la - lb;
+        const T adL = dL < T(0) ? -dL : dL;
+        const T h = (la > lb ? la : lb) - (zea > zeb ? zea : zeb);
+        dd = dd || adL < k.tau_l || h < k.tau_h;
+        dead[f] = dd;
+        pos[f] = dL > T(0);
+        hf[f] = dd ? T(1) : h;
+        aL[f] = dd ? T(1) : adL;
+        nf[f] = dd ? T(1) : (n < T(1e-12) ? T(1e-12) : n);
+        if (M::cbrt_try(hf[f], cb[f], ce[f]))
+            settle |= 1u << f;
+    }
+    if (settle) {
+#pragma unroll
+        for (int f = 0; f < NF; f++)
+            if (settle & (1u << f))
+                cb[f] = M::cbrt_settle(hf[f], cb[f], ce[f]);
+    }
+    T v[NF];
+    unsigned capv = 0u;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        const T S = M::div_c(aL[f], d[f], rd[f]);
+        v[f] = M::rcp_bf(nf[f]) * cb[f] * M::sqrt_bf(S);
+        if (M::caps(v[f], k.g, hf[f]))
+            capv |= 1u << f;
+    }
+    if (capv) {
+#pragma unroll
+        for (int f = 0; f < NF; f++)
+            if (capv & (1u << f))
+                v[f] = M::vcr(k.g, hf[f]);
+    }
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        T Qm = v[f] * hf[f] * k.w;
+        const T Qc = M::div_c(aL[f] * k.A, k.den, k.rden);
+        const bool c = Qc < Qm;
+        Qm = c ? Qc : Qm;
+        cap[f] = (!dead[f] && c) ? 1u : 0u;
+        Q[f] = dead[f] ? T(0) : (pos[f] ? Qm : -Qm);
+    }
+}
+
+// Limiter without branches (physics.h:127-134): hold/out when the outflow
+// volume exceeds the held volume, else 1.
+template <typename T, int MATH>
+__device__ __forceinline__ T limiter_bf(T out_vol, T h, T A)
+{
+    using M = Mth<T, MATH>;
+    const T hold = h * A;
+    const bool lim = out_vol > hold && out_vol > T(0);
+    const T o = lim ? out_vol : T(1);
+    const T q = M::div_c(hold, o, M::rcp_bf(o));
+    return lim ? q : T(1);
 }
 
 // Open-edge discharge to the virtual neighbour z - S_bnd*dx, h = 0, same n,

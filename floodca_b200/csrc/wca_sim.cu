@@ -61,6 +61,17 @@ __global__ void k_fill_interior(void *p, long long pitch, int nr, int nc, double
     }
 }
 
+__global__ void k_fill_all(void *p, long long n, double v, int esize)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (esize == 8)
+            static_cast<double *>(p)[i] = v;
+        else
+            static_cast<float *>(p)[i] = (float)v;
+    }
+}
+
 // Writes C*Rday (rounded in the element type, as the reference's
 // C[a]*Rday[a]*F multiplies left to right) into the padded field `cr` and
 // tracks the minimum and maximum over LAND cells as order-preserving keys,
@@ -416,6 +427,17 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
         mh = probe.data();
     }
     const int has_sea = memchr(mh, M_SEA, (size_t)N) != nullptr;
+    // all-LAND grids use the mask-free kernel: padding elevation PAD_Z makes
+    // every face to the padding carry zero discharge (needs tau_h > 0)
+    bool all_land = c.tau_h > 0.0;
+    for (long long i = 0; i < N && all_land; i++)
+        all_land = mh[i] == M_LAND;
+    s->landonly = all_land;
+    if (all_land) {
+        k_fill_all<<<1024, 256, 0, s->stream>>>(s->z, (long long)s->nelem, PAD_Z, (int)es);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(put_field(s, s->z, z, es, kind));
+    }
     int inflow_ok = 0;
     if (c.inflow_cell >= 0 && c.inflow_cell < N)
         inflow_ok = mh[c.inflow_cell] == M_LAND;
@@ -480,6 +502,7 @@ static int resolve_variant(FcabSim *s)
     key.cpl = s->cpl;
     key.math = s->cfg.precision == FCAB_PREC_F32 ? s->cfg.math : FCAB_MATH_EXACT;
     key.rainf = s->rain_field ? 1 : 0;
+    key.landonly = s->landonly ? 1 : 0;
     bool ok = key.prec == FCAB_PREC_F32 ? lookup_f32(key, &s->L)
               : key.prec == FCAB_PREC_F32_ALL ? lookup_f32all(key, &s->L)
                                                : lookup_f64(key, &s->L);
@@ -775,6 +798,7 @@ extern "C" int fcab_sim_info(FcabSim *s, FcabInfo *info)
     info->warps = s->warps_total;
     info->ctas_per_sm = s->occupancy;
     info->rain_field = s->rain_field ? 1 : 0;
+    info->land_only = s->landonly ? 1 : 0;
     info->land_cells = s->land_cells;
     info->faces_per_step = s->faces_per_step;
     info->pitch = s->pitch;
@@ -939,8 +963,22 @@ __global__ void k_math_probe(int which, const float *x, const float *y, float *o
             r = cbrt_sq_rn(x[i]);
         else if (which == 1)
             r = min_vcr_rn(x[i], g, y[i]);
-        else
+        else if (which == 2)
             r = Mth<float, MATH_FAST>::cbrt_sq(x[i]);
+        else if (which == 3)
+            r = (__fsqrt_rn(x[i]) == sqrt_nr(x[i])) && (__frcp_rn(x[i]) == rcp_nr(x[i])) ? 1.f : 0.f;
+        else if (which == 4)
+            r = rcp_nr(x[i]);
+        else if (which == 5)
+            r = sqrt_nr(x[i]);
+        else if (which == 6)
+            r = div_mk(x[i], y[i], __frcp_rn(y[i]));
+        else if (which == 7)
+            r = __frcp_rn(x[i]);
+        else if (which == 8)
+            r = __fsqrt_rn(x[i]);
+        else
+            r = __fdiv_rn(x[i], y[i]);
         out[i] = r;
     }
 }

@@ -26,6 +26,7 @@ struct FcabSim {
     fcab::RunK<double> rkd;
     fcab::TimeCfg tc;
     bool rain_field = false;
+    bool landonly = false;       // mask-free kernel variant (all cells LAND)
     int cpl = 2, grid = 1, warps_total = 4, occupancy = 1;
     fcab::Launchers L;
     bool have_variant = false, variant_dirty = true;

@@ -208,7 +208,7 @@ typedef struct FcabPoll {
 
 /* Launch shape chosen for a session. */
 typedef struct FcabInfo {
-    int cols_per_lane, grid, warps, ctas_per_sm, rain_field;
+    int cols_per_lane, grid, warps, ctas_per_sm, rain_field, land_only;
     long long land_cells, faces_per_step, pitch;
 } FcabInfo;
 
@@ -281,9 +281,11 @@ FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uin
 /* The session's cudaStream_t. */
 FCAB_API void *fcab_sim_stream(FcabSim *s);
 
-/* Test hook: evaluates a device math helper on n host inputs (which = 0:
- * RN(cbrt(x*x)) as the exact mode computes hf^(2/3); 1: min(x, RN(sqrt(g*y)));
- * 2: the fast-mode hf^(2/3)) and writes n host outputs. */
+/* Test hook: evaluates a device math helper on n host inputs and writes n
+ * host outputs. which = 0: RN(cbrt(x*x)) as the exact mode computes
+ * hf^(2/3); 1: min(x, RN(sqrt(g*y))); 2: the fast-mode hf^(2/3); 4/5/6: the
+ * branch-free reciprocal, square root and Markstein quotient x/y; 7/8/9: the
+ * IEEE reciprocal, square root and quotient they must equal. */
 FCAB_API int fcab_math_probe(int which, const float *x, const float *y, float *out, long long n,
                              float g);
 

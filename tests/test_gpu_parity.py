@@ -58,11 +58,17 @@ def test_strip_widths_agree(case, cpl):
     _compare(r, f, "f32", case)
 
 
+# Cases the reference-facing ABI can express (no rain_end, no point inflow:
+# FcaRunCfg has no fields for them).
+DROPIN_CASES = ["mixed_k4", "mixed_k8", "mixed_k8_open", "tiny_1x7", "tiny_3x3", "column_k8",
+                "lambda", "forcing"]
+
+
 @pytest.mark.parametrize("kind", ["f32", "f64"])
-@pytest.mark.parametrize("case", ["c1_64", "mixed_k4", "mixed_k8", "tiny_1x7", "column_k8",
-                                  "lambda", "forcing"])
+@pytest.mark.parametrize("case", DROPIN_CASES)
 def test_dropin_abi_matches_reference(case, kind):
     d, p, f, force = load_case(GOLDEN / f"{case}.npz")
+    assert p.rain_end <= 0 and p.inflow_cell < 0
     g = DropinGrid(d, p, double=(kind == "f64"))
     with tempfile.TemporaryDirectory() as tmp:
         if force is not None:
@@ -114,3 +120,31 @@ def test_device_critical_velocity_min_is_exact():
     vcr = np.sqrt(np.float64(np.float32(9.81)) * h.astype(np.float64)).astype(np.float32)
     want = np.where(v > vcr, vcr, v)
     assert np.array_equal(out, want)
+
+
+def test_branch_free_ops_equal_ieee():
+    """The branch-free reciprocal, square root and Markstein quotient used by
+    the exact kernels equal CUDA's IEEE operations: every float of two
+    binades (both exponent parities for the square root), and random
+    quotients including the fixed divisors the kernels use."""
+    from floodca_b200.lib import core
+    L = core()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+
+    def run(which, x, y=None):
+        out = np.empty_like(x)
+        assert L.fcab_math_probe(which, vp(x), None if y is None else vp(y), vp(out), x.size,
+                                 9.81) == 0
+        return out
+
+    mant = np.arange(0, 1 << 23, dtype=np.uint32)
+    for e in (127, 128, 110):
+        x = ((np.uint32(e) << 23) | mant).view(np.float32)
+        assert np.array_equal(run(4, x), run(7, x))
+        assert np.array_equal(run(5, x), run(8, x))
+    rng = np.random.default_rng(3)
+    for b0 in (None, 90.0, 8100.0):
+        a = (rng.uniform(-1, 1, 1 << 22) * 2.0 ** rng.uniform(-30, 30, 1 << 22)).astype(np.float32)
+        b = (np.full(a.size, b0, np.float32) if b0 else
+             (2.0 ** rng.uniform(-30, 30, a.size)).astype(np.float32))
+        assert np.array_equal(run(6, a, b), run(9, a, b))

@@ -531,6 +531,7 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
         int ko1[CPL];                        // open sides of row i-2
         T L3[CPL], L4[CPL];                  // new level (NaN: WALL) of rows i-3, i-4
         T hn3[CPL];                          // new depth of row i-3
+        unsigned eflag = 0u;                 // stage-E candidates of row i-3 (bit per column)
         T hm[CPL];                           // hmax of row i-2
         T cr1[CPL];                          // rain field of row i-2
 #pragma unroll
@@ -693,6 +694,7 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                 }
             }
 
+            unsigned eflag_next = 0u;
             // ---- D: limiter-scaled net inflow and depth update of row i-2
             //      (s0: row i-1 below, s1: the row itself, s2: row i-3 above)
             T hn2[CPL], Ln2[CPL];
@@ -722,8 +724,22 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                 }
                 const bool sea_on = rk.has_sea != 0;
                 const bool inflow_row = r == rk.inflow_r;
+                // open-edge terms exist only on open edge rows or edge lanes
+                const bool open2 = edge_lane || (rk.open && ((r == 0 && rk.edge_n) ||
+                                                             (r == nr - 1 && rk.edge_s)));
+                const bool row2_in = r >= 0 && r < nr;
+                // stage-E threshold: the warp's running velocity maximum
+                const T thr = want_v ? warp_max_nonneg(vmax) : T(0);
                 T *tm_row = g.tmax + (long long)(r + PADR) * g.pitch + colo;
-                bool rose_any = false;
+                bool rose_any = false, bnd_open = false;
+                T qbnd[CPL];
+                if constexpr (LANDONLY && sizeof(AccT) == 8 && !RAINF) {
+                    if (row2_out && out_lane) {
+#pragma unroll
+                        for (int j = 0; j < CPL; j++)
+                            rain_cells += colok[j] ? 1 : 0;
+                    }
+                }
                 T hmx[CPL];
 #pragma unroll
                 for (int j = 0; j < CPL; j++) {
@@ -786,51 +802,61 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                             Qs < T(0))
                             sea += (double)dt * (double)(-Qs);
                     }
-                    const T Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
-                    net -= Qo;
-                    T ha = p2.h[j];
+                    T Qo = T(0);
+                    if (open2) {
+                        Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
+                        net -= Qo;
+                    }
                     const bool cell_out = row2_out && out_lane && colok[j];
-                    if (land) {
-                        const T rain = RAINF ? cr1[j] * F : rainv;
-                        ha = ha + (dt * Mth<T, MATH>::div_c(net, A, k.inv_A) + rain);
-                        if (cell_out) {
-                            // sum(A*rain) = A*sum(rain): A*rain is exact in double
-                            if constexpr (sizeof(AccT) == 4)
-                                a_rain += A * rain;
-                            else if constexpr (RAINF)
-                                rain_sum += (double)rain;
-                            else
-                                rain_cells += 1;
-                        }
-                        if (ha < T(0)) {
-                            if (cell_out)
-                                a_clamp += acc_mul<AccT, T>(-ha, A);
-                            ha = T(0);
-                        }
-                        if (inflow_row && cbase + j == rk.inflow_c)
-                            ha = ha + inflow_dh;
+                    T ha = p2.h[j];
+                    const T rain = RAINF ? cr1[j] * F : rainv;
+                    T hu = ha + (dt * Mth<T, MATH>::div_c(net, A, k.inv_A) + rain);
+                    hu = land ? hu : ha;
+                    // rare events are settled after the loop: clamp, open edge, sea
+                    if (land && hu < T(0)) {
+                        if (cell_out)
+                            a_clamp += acc_mul<AccT, T>(-hu, A);
+                        hu = T(0);
                     }
-                    if (cell_out) {
-                        if (sea_on)
-                            a_sea += (AccT)sea;
-                        if (ko1[j])
-                            a_bnd += acc_mul<AccT, T>(dt, Qo);
+                    ha = hu;
+                    if (inflow_row && land && cbase + j == rk.inflow_c)
+                        ha = ha + inflow_dh;
+                    if constexpr (sizeof(AccT) == 4) {
+                        if (cell_out && land)
+                            a_rain += A * rain;
+                    } else if constexpr (RAINF) {
+                        rain_sum += (cell_out && land) ? (double)rain : 0.0;
+                    } else if constexpr (!LANDONLY) {
+                        rain_cells += (cell_out && land) ? 1 : 0;
                     }
+                    if (sea_on && cell_out)
+                        a_sea += (AccT)sea;
+                    if (open2)
+                        bnd_open |= cell_out && ko1[j] != 0;
+                    qbnd[j] = Qo;
                     if constexpr (LANDONLY) {
                         // outside the grid: keep the padding depth, no face
-                        const bool inside = colok[j] && p2.z[j] < T(0.5 * PAD_Z);
+                        const bool inside = colok[j] && row2_in;
                         hn2[j] = inside ? ha : p2.h[j];
                         Ln2[j] = inside ? p2.z[j] + ha : qnan;
                     } else {
                         hn2[j] = ha;
                         Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
                     }
-                    hmx[j] = hm[j];
-                    if (cell_out && land && ha > hm[j]) {
-                        hmx[j] = ha;
-                        rose_any = true;
+                    if (want_v && cell_out && land && ha >= k.tau_h &&
+                        !(thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, ha)))
+                        eflag_next |= 1u << j;
+                    const bool rise = cell_out && land && ha > hm[j];
+                    hmx[j] = rise ? ha : hm[j];
+                    rose_any |= rise;
+                    if (rise)
                         tm_row[j] = tmax_val;
-                    }
+                }
+                if (bnd_open) {
+#pragma unroll
+                    for (int j = 0; j < CPL; j++)
+                        if (row2_out && out_lane && colok[j] && ko1[j])
+                            a_bnd += acc_mul<AccT, T>(dt, qbnd[j]);
                 }
                 if (row2_out && out_lane) {
                     const long long off2 = (long long)(r + PADR) * g.pitch + colo;
@@ -841,12 +867,13 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
             }
 
             // ---- E: next step's stable velocity of row i-3 from the new
-            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2). Cells whose
-            //      critical velocity cannot exceed the warp's running maximum
-            //      are skipped (their velocity is capped by it).
-            if (want_v) {
+            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2), for the
+            //      cells stage D flagged: wet LAND output cells whose critical
+            //      velocity could exceed the warp's running maximum (every
+            //      other cell's velocity is capped below it).
+            if (want_v && __any_sync(0xffffffffu, eflag != 0u)) {
                 const int r = i - 3;
-                const T thr = warp_max_nonneg(vmax);
+                vmax = warp_max_nonneg(vmax);
                 const T Ll = sh_up(L3[CPL - 1]), Lr = sh_dn(L3[0]);
                 T L2l = T(0), L2r = T(0), L4l = T(0), L4r = T(0);
                 if constexpr (K == 8) {
@@ -856,41 +883,48 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                     L4r = sh_dn(L4[0]);
                 }
                 const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
-                if (r >= r0 && r < r1 && out_lane) {
 #pragma unroll
-                    for (int j = 0; j < CPL; j++) {
-                        const T hv = hn3[j];
-                        if (p3.m[j] != M_LAND || !colok[j] || !(hv >= k.tau_h))
-                            continue;
-                        if (thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, hv))
-                            continue;
-                        const int c = cbase + j;
-                        const T la = L3[j];
-                        T mo = T(0);
-                        mo = fmax(mo, fabs(la - right_of<T, CPL>(L3, j, Lr)));
-                        mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
-                        mo = fmax(mo, fabs(la - Ln2[j]));
-                        mo = fmax(mo, fabs(la - L4[j]));
-                        if (edge_row || (edge_lane && rk.open &&
-                                         ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e)))) {
-                            const T lv = p3.z[j] - k.S_bnd * k.dx;
-                            mo = fmax(mo, fabs(la - lv));
-                        }
-                        T Smax = Mth<T, MATH>::div(mo, k.dx);
-                        if constexpr (K == 8) {
-                            T md = T(0);
-                            md = fmax(md, fabs(la - right_of<T, CPL>(Ln2, j, L2r)));
-                            md = fmax(md, fabs(la - left_of<T, CPL>(Ln2, j, L2l)));
-                            md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
-                            md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
-                            const T Sd = Mth<T, MATH>::div(md, dd);
-                            if (Sd > Smax)
-                                Smax = Sd;
-                        }
-                        const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
-                        if (v > vmax)
-                            vmax = v;
+                for (int j = 0; j < CPL; j++) {
+                    if (!(eflag & (1u << j)))
+                        continue;
+                    const T hv = hn3[j];
+                    const int c = cbase + j;
+                    const T la = L3[j];
+                    T mo = T(0);
+                    mo = fmax(mo, fabs(la - right_of<T, CPL>(L3, j, Lr)));
+                    mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
+                    mo = fmax(mo, fabs(la - Ln2[j]));
+                    mo = fmax(mo, fabs(la - L4[j]));
+                    if (edge_row || (edge_lane && rk.open &&
+                                     ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e)))) {
+                        const T lv = p3.z[j] - k.S_bnd * k.dx;
+                        mo = fmax(mo, fabs(la - lv));
                     }
+                    T md = T(0);
+                    if constexpr (K == 8) {
+                        md = fmax(md, fabs(la - right_of<T, CPL>(Ln2, j, L2r)));
+                        md = fmax(md, fabs(la - left_of<T, CPL>(Ln2, j, L2l)));
+                        md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
+                        md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
+                    }
+                    // cheap upper bound first; the exact velocity only when
+                    // it could raise the running maximum
+                    T Sb = mo * k.rdx;
+                    if constexpr (K == 8) {
+                        const T sd = md * k.rdd;
+                        Sb = sd > Sb ? sd : Sb;
+                    }
+                    if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <= vmax)
+                        continue;
+                    T Smax = Mth<T, MATH>::div(mo, k.dx);
+                    if constexpr (K == 8) {
+                        const T Sd = Mth<T, MATH>::div(md, dd);
+                        if (Sd > Smax)
+                            Smax = Sd;
+                    }
+                    const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
+                    if (v > vmax)
+                        vmax = v;
                 }
             }
 
@@ -914,6 +948,7 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
                 L4[j] = L3[j];
                 L3[j] = Ln2[j];
                 hn3[j] = hn2[j];
+                eflag = eflag_next;
                 if (row1_out && out_lane)
                     hm[j] = hm_next[j];
                 if constexpr (RAINF)

@@ -207,8 +207,9 @@ __device__ __forceinline__ void faces_q(const T (&za)[NF], const T (&ha)[NF], co
                                         unsigned (&cap)[NF])
 {
     using M = Mth<T, MATH>;
-    T hf[NF], aL[NF], nf[NF], cb[NF], ce[NF];
-    bool dead[NF], pos[NF];
+    // sL: signed level difference of a live face, 0 for a face that carries
+    // no flow (so no boolean state crosses the phases)
+    T hf[NF], sL[NF], nf[NF], cb[NF], ce[NF];
     unsigned settle = 0u;
 #pragma unroll
     for (int f = 0; f < NF; f++) {
@@ -231,14 +232,13 @@ __device__ __forceinline__ void faces_q(const T (&za)[NF], const T (&ha)[NF], co
             dd = dd || ((la - lb) > T(0) ? sa : sb);
         }
         const T dL = la - lb;
-        const T adL = dL < T(0) ? -dL : dL;
         const T h = (la > lb ? la : lb) - (zea > zeb ? zea : zeb);
-        dd = dd || adL < k.tau_l || h < k.tau_h;
-        dead[f] = dd;
-        pos[f] = dL > T(0);
+        dd = dd || fabs(dL) < k.tau_l || h < k.tau_h;
+        // a dead face's hf is replaced so the cube root stays on its fast
+        // path; its other operands may produce NaN, which the final select drops
         hf[f] = dd ? T(1) : h;
-        aL[f] = dd ? T(1) : adL;
-        nf[f] = dd ? T(1) : (n < T(1e-12) ? T(1e-12) : n);
+        sL[f] = dd ? T(0) : dL;
+        nf[f] = n < T(1e-12) ? T(1e-12) : n;
         if (M::cbrt_try(hf[f], cb[f], ce[f]))
             settle |= 1u << f;
     }
@@ -252,7 +252,7 @@ __device__ __forceinline__ void faces_q(const T (&za)[NF], const T (&ha)[NF], co
     unsigned capv = 0u;
 #pragma unroll
     for (int f = 0; f < NF; f++) {
-        const T S = M::div_c(aL[f], d[f], rd[f]);
+        const T S = M::div_c(fabs(sL[f]), d[f], rd[f]);
         v[f] = M::rcp_bf(nf[f]) * cb[f] * M::sqrt_bf(S);
         if (M::caps(v[f], k.g, hf[f]))
             capv |= 1u << f;
@@ -266,11 +266,32 @@ __device__ __forceinline__ void faces_q(const T (&za)[NF], const T (&ha)[NF], co
 #pragma unroll
     for (int f = 0; f < NF; f++) {
         T Qm = v[f] * hf[f] * k.w;
-        const T Qc = M::div_c(aL[f] * k.A, k.den, k.rden);
+        const T Qc = M::div_c(fabs(sL[f]) * k.A, k.den, k.rden);
         const bool c = Qc < Qm;
         Qm = c ? Qc : Qm;
-        cap[f] = (!dead[f] && c) ? 1u : 0u;
-        Q[f] = dead[f] ? T(0) : (pos[f] ? Qm : -Qm);
+        const bool live = sL[f] != T(0);
+        cap[f] = (live && c) ? 1u : 0u;
+        Q[f] = live ? copysign(Qm, sL[f]) : T(0);
+    }
+}
+
+// Upper bound of cell_velocity (relative error of the float approximations
+// below 1e-5): max(min(h^(2/3) sqrt(S) / n, sqrt(g h)), 1e-6) * (1 + 1e-4).
+template <typename T>
+__device__ __forceinline__ T cell_velocity_bound(T h, T n, T S, const StepK<T> &k)
+{
+    if constexpr (sizeof(T) == 4) {
+        const float nn = n < 1e-12f ? 1e-12f : n;
+        const float cb = ex2_approx(lg2_approx(h) * 0.666666687f);
+        const float sq = S > 0.0f ? S * rsqrt_approx(S) : 0.0f;
+        float v = rcp_approx(nn) * cb * sq;
+        const float p = k.g * h;
+        const float vc = p * rsqrt_approx(p);
+        v = v < vc ? v : vc;
+        v = v < 1e-6f ? 1e-6f : v;
+        return v * 1.0001f;
+    } else {
+        return T(1e300);   // no bound: the FP64 kernels evaluate every candidate
     }
 }
 
@@ -302,13 +323,12 @@ template <typename T>
 __device__ __forceinline__ T open_sum(T q, int kcnt)
 {
     T s = kcnt > 0 ? q : T(0);
-    if (kcnt > 1)
-        s = s + q;
-    if (kcnt > 2)
-        s = s + q;
-    if (kcnt > 3)
-        s = s + q;
-    return s;
+    const T s2 = s + q;
+    s = kcnt > 1 ? s2 : s;
+    const T s3 = s + q;
+    s = kcnt > 2 ? s3 : s;
+    const T s4 = s + q;
+    return kcnt > 3 ? s4 : s;
 }
 
 // Limiter (physics.h:127-134).

@@ -1009,3 +1009,27 @@ done:
     cudaFree(dout);
     return rc;
 }
+
+namespace fcab {
+
+// Run constants of an FP32 configuration, for entry points that launch the
+// step kernels without a session.
+void make_run_params_f32(const FcabConfig &cfg, RunK<float> *rk, TimeCfg *tc)
+{
+    fill_runk<float>(*rk, cfg);
+    memset(tc, 0, sizeof(*tc));
+    const int p = cfg.precision;
+    tc->T_sim = as_real(cfg.T_sim, p);
+    tc->out_every = as_real(cfg.out_every, p);
+    tc->D_h = as_real(cfg.D_h, p);
+    tc->phi = as_real(cfg.phi, p);
+    tc->rain_end = cfg.rain_end;
+    tc->inflow_peak = cfg.inflow_peak;
+    tc->inflow_t_peak = cfg.inflow_t_peak;
+    tc->inflow_t_end = cfg.inflow_t_end;
+    tc->hyeto = cfg.hyeto;
+    tc->max_steps = cfg.max_steps;
+    tc->U = cfg.U > 0 ? cfg.U : 1;
+}
+
+}  // namespace fcab

@@ -38,3 +38,10 @@ struct FcabSim {
     double V0 = 0.0;
     long long land_cells = 0, open_faces = 0, faces_per_step = 0;
 };
+
+namespace fcab {
+// Records the calling thread's fcab_last_error() message (wca_sim.cu).
+void set_error(const char *msg);
+// Run constants of an FP32 configuration (defined in wca_sim.cu).
+void make_run_params_f32(const FcabConfig &cfg, RunK<float> *rk, TimeCfg *tc);
+}  // namespace fcab

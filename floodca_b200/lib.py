@@ -62,6 +62,8 @@ def core() -> C.CDLL:
         "fcab_sim_stream": (_P, [_P]),
         "fcab_sim_destroy": (None, [_P]),
         "fcab_math_probe": (C.c_int, [C.c_int, _P, _P, _P, C.c_longlong, C.c_float]),
+        "fcab_run_noalloc": (C.c_int, [C.POINTER(FcabConfig), _P, _P, _P, _P, _P, _P, _P, _P,
+                                       _P, C.POINTER(FcabStats)]),
         "fcab_last_error": (C.c_char_p, []),
         "fcab_version": (C.c_char_p, []),
     }

@@ -281,6 +281,28 @@ FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uin
 /* The session's cudaStream_t. */
 FCAB_API void *fcab_sim_stream(FcabSim *s);
 
+/* Runs cfg->max_steps steps of the FP32 WCA step (the same fused kernel as
+ * the sessions) on caller-owned device arrays, allocating nothing. No
+ * counterpart in the reference. For callers that cannot call cudaMalloc:
+ * processes whose device memory belongs to another allocator (a framework's
+ * pool, an arena sized at start-up), or pipelines that must not allocate once
+ * running, since cudaMalloc/cudaFree synchronise the device and stall other
+ * streams. The working memory is one library-global device array of 2^19
+ * padded cells (about 15 MB, held on every GPU that loads the library until
+ * exit): (nrows + 8) * round_up(ncols + 132, 32) must not exceed 524288
+ * (e.g. 512 x 768), else FCAB_ERR_ARG. Inputs z, n, mask (row-major
+ * nrows*ncols, device), optional C and Rday (NULL: no rain); h and hmax are
+ * read as the initial state and overwritten with the final state, tmax too
+ * (NULL: start at 0, not written back). stream: cudaStream_t, NULL for the
+ * legacy stream. stats (host, may be NULL) receives the run totals after a
+ * stream synchronisation. The first call on each device looks up the array's
+ * device address; make that first call before any stream capture. Calls
+ * share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race and corrupt each other. */
+FCAB_API int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const float *n,
+                              const float *C, const float *Rday, const uint8_t *mask, float *h,
+                              float *hmax, float *tmax, void *stream, FcabStats *stats);
+
 /* Test hook: evaluates a device math helper on n host inputs and writes n
  * host outputs. which = 0: RN(cbrt(x*x)) as the exact mode computes
  * hf^(2/3); 1: min(x, RN(sqrt(g*y))); 2: the fast-mode hf^(2/3); 4/5/6: the

@@ -158,6 +158,38 @@ CASES = {
 }
 
 
+# The isotropy protocol of the reference's analysis/e9_aniso.py, reduced: a
+# flat plane at 90 m, closed, no rain, a 5x5 column of 1 m, runs of CHUNK
+# steps each restarted from the float32 depth (hmax = h, t = 0), FP64.
+E9_SMALL = {"n": 512, "chunk": 400, "chunks": 30, "thresh": 1e-3}
+
+
+def e9_domain(n):
+    z = np.full((n, n), 10.0, np.float32)
+    h = np.zeros((n, n), np.float32)
+    c = n // 2
+    h[c - 2:c + 3, c - 2:c + 3] = 1.0
+    return Domain(z=z, mask=np.zeros((n, n), np.uint8), n=np.full((n, n), 0.03, np.float32),
+                  C=np.zeros((n, n), np.float32), Rday=np.zeros((n, n), np.float32), h=h, dx=90.0)
+
+
+def make_e9_small(K):
+    """Wet-cell counts after every chunk and the final float32 depth, from
+    the reference core in FP64."""
+    n, chunk = E9_SMALL["n"], E9_SMALL["chunk"]
+    d = e9_domain(n)
+    p = RunParams(K=K, U=1, boundary="closed", steps=chunk)
+    h32 = d.h.copy()
+    wet = []
+    for _ in range(E9_SMALL["chunks"]):
+        dd = Domain(z=d.z, mask=d.mask, n=d.n, C=d.C, Rday=d.Rday, h=h32, dx=d.dx)
+        r = refcore.run(dd, p, "f64")
+        h32 = np.asarray(r["h"], np.float64).astype(np.float32)
+        wet.append(int((np.asarray(r["h"], np.float64) > E9_SMALL["thresh"]).sum()))
+    return {"wet": np.asarray(wet, np.int64), "h_final": h32, "K": np.int64(K),
+            "params": json.dumps(E9_SMALL)}
+
+
 def write_forcing(days, tmp: Path) -> list[str]:
     files = []
     for i, r in enumerate(days):
@@ -210,9 +242,13 @@ def main() -> int:
     if not refcore.build(a.ref):
         print(f"reference sources not found under {a.ref}", file=sys.stderr)
         return 1
-    for name in a.cases or CASES:
+    for name in [c for c in (a.cases or CASES) if c in CASES]:
         np.savez_compressed(HERE / f"{name}.npz", **make_case(name))
         print("wrote", name)
+    if not a.cases or "e9" in a.cases:
+        for K in (4, 8):
+            np.savez_compressed(HERE / f"e9_small_k{K}.npz", **make_e9_small(K))
+            print("wrote e9_small", K)
     # ABI layout of the reference structs, from oracle/_ref/abi_probe_*
     import subprocess
     layout = {k: json.loads(subprocess.check_output([str(refcore.REF_DIR / f"abi_probe_{k}")]))

@@ -141,3 +141,9 @@ class FcabInfo(C.Structure):
                 ("ctas_per_sm", C.c_int), ("rain_field", C.c_int), ("land_only", C.c_int),
                 ("land_cells", C.c_longlong), ("faces_per_step", C.c_longlong),
                 ("pitch", C.c_longlong)]
+
+
+class FcabBatchInfo(C.Structure):
+    _fields_ = [("members", C.c_int), ("cols_per_lane", C.c_int), ("seg_rows", C.c_int),
+                ("grid", C.c_int), ("total_units", C.c_int), ("launches", C.c_longlong),
+                ("windows", C.c_longlong), ("graph_replays", C.c_longlong)]

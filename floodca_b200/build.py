@@ -32,8 +32,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC)]
 
-CORE_SRCS = ["wca_inst_f32.cu", "wca_inst_f32all.cu", "wca_inst_f64.cu", "wca_sim.cu",
-             "wca_noalloc.cu"]
+CORE_SRCS = ["wca_inst_f32.cu", "wca_inst_f32all.cu", "wca_inst_f64.cu", "wca_inst_batch.cu",
+             "wca_sim.cu", "wca_noalloc.cu", "wca_batch.cu"]
 
 
 def _deps_newer(obj: Path, srcs: list[Path]) -> bool:

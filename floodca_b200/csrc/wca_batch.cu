@@ -1,0 +1,260 @@
+// Batched ensemble runs (fcab_batch_*): many sessions advanced together.
+//
+// Each member is an ordinary session (own padded grid, control block, dt,
+// time, rain). A batched launch advances every active member by one step
+// (k_step_batch); a CUDA graph of `graph_steps` launches is replayed until
+// every member has reached the end of the current output window or of its
+// run, then the next window opens (k_batch_window). The host reads one
+// gathered activity flag per member between graph replays.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "floodca_b200.h"
+#include "wca_dispatch.h"
+#include "wca_sim_internal.h"
+
+using namespace fcab;
+
+namespace {
+
+__global__ void k_gather_active(const MemberD<float> *members, int n, int *flags)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n) {
+        const Ctl *c = members[m].ctl;
+        flags[m] = c->active ? 1 : (c->done ? 0 : 2);   // 1 running, 2 paused, 0 done
+    }
+}
+
+int bfail(int code, const char *msg)
+{
+    set_error(msg);
+    return code;
+}
+
+}  // namespace
+
+struct FcabBatch {
+    std::vector<FcabSim *> members;
+    int n = 0;
+    cudaStream_t stream = nullptr;
+    VariantKey key{};
+    BatchLaunchers L{};
+    MemberD<float> *d_members = nullptr;
+    int *d_unit_member = nullptr;
+    BatchQ *d_q = nullptr;
+    int *d_flags = nullptr;
+    int *h_flags = nullptr;     // pinned
+    int total_units = 0, grid = 1, seg = 64;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long long launches = 0, windows = 0, replays = 0;
+};
+
+extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n,
+                                 int cols_per_lane, int seg_rows, const int *member_seg_rows,
+                                 void *stream)
+{
+    *out = nullptr;
+    if (n < 1 || !members)
+        return bfail(FCAB_ERR_ARG, "fcab_batch_create: no members");
+    FcabSim *m0 = members[0];
+    for (int i = 0; i < n; i++) {
+        const FcabSim *s = members[i];
+        if (!s || !s->inited)
+            return bfail(FCAB_ERR_STATE, "fcab_batch_create: member not uploaded");
+        if (s->cfg.precision != FCAB_PREC_F32 || s->cfg.K != m0->cfg.K ||
+            s->cfg.math != m0->cfg.math || s->landonly != m0->landonly ||
+            s->rain_field != m0->rain_field || s->dev != m0->dev)
+            return bfail(FCAB_ERR_ARG, "fcab_batch_create: members must share FP32 precision, K, "
+                                       "math, rain form, mask form and device");
+        if (s->tc.n_force_days > 0 || s->tc.progress_every > 0)
+            return bfail(FCAB_ERR_ARG, "fcab_batch_create: members with forcing days or "
+                                       "progress pauses run as single sessions");
+    }
+    FcabBatch *b = new FcabBatch();
+    b->members.assign(members, members + n);
+    b->n = n;
+    b->stream = stream ? (cudaStream_t)stream : m0->stream;
+    b->key.prec = FCAB_PREC_F32;
+    b->key.K = m0->cfg.K;
+    b->key.cpl = (cols_per_lane == 1 || cols_per_lane == 2 || cols_per_lane == 4) ? cols_per_lane : 2;
+    if (b->key.K == 8 && b->key.cpl == 4)
+        b->key.cpl = 2;
+    b->key.math = m0->cfg.math;
+    b->key.rainf = m0->rain_field ? 1 : 0;
+    b->key.landonly = m0->landonly ? 1 : 0;
+    if (!lookup_batch_f32(b->key, &b->L)) {
+        delete b;
+        return bfail(FCAB_ERR_ARG, "fcab_batch_create: no compiled batch variant");
+    }
+    b->seg = seg_rows > 0 ? seg_rows : 64;
+    const int ow = 32 * b->key.cpl - 2 * (b->key.cpl == 1 ? 3 : 4);
+    std::vector<MemberD<float>> md(n);
+    std::vector<int> um;
+    for (int i = 0; i < n; i++) {
+        FcabSim *s = members[i];
+        MemberD<float> &d = md[i];
+        d.g.z = (const float *)s->z;
+        d.g.n = (const float *)s->n;
+        d.g.cr = s->rain_field ? (const float *)s->cr : nullptr;
+        d.g.m = s->m;
+        d.g.h0 = (float *)s->h0;
+        d.g.h1 = (float *)s->h1;
+        d.g.hmax = (float *)s->hmax;
+        d.g.tmax = (float *)s->tmax;
+        d.g.pitch = s->pitch;
+        d.g.nr = s->cfg.nrows;
+        d.g.nc = s->cfg.ncols;
+        d.rk = s->rkf;
+        d.tc = s->tc;
+        d.ctl = s->ctl;
+        d.strips = (s->cfg.ncols + ow - 1) / ow;
+        d.seg = member_seg_rows && member_seg_rows[i] > 0 ? member_seg_rows[i] : b->seg;
+        const int blocks = (s->cfg.nrows + d.seg - 1) / d.seg;
+        d.units = d.strips * blocks;
+        d.unit_off = (int)um.size();
+        um.insert(um.end(), (size_t)d.units, i);
+    }
+    b->total_units = (int)um.size();
+    cudaError_t e = cudaMalloc(&b->d_members, sizeof(MemberD<float>) * n);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_unit_member, sizeof(int) * um.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_q, sizeof(BatchQ));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_flags, sizeof(int) * n);
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_flags, sizeof(int) * n);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_members, md.data(), sizeof(MemberD<float>) * n,
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_unit_member, um.data(), sizeof(int) * um.size(),
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(b->d_q, 0, sizeof(BatchQ), b->stream);
+    int nsm = 1, per_sm = 1;
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m0->dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->L.step_fn, 128, 0);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        fcab_batch_destroy(b);
+        return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+    }
+    b->grid = nsm * (per_sm > 0 ? per_sm : 1);
+    *out = b;
+    return 0;
+}
+
+extern "C" void fcab_batch_destroy(FcabBatch *b)
+{
+    if (!b)
+        return;
+    if (b->graph)
+        cudaGraphExecDestroy(b->graph);
+    cudaFree(b->d_members);
+    cudaFree(b->d_unit_member);
+    cudaFree(b->d_q);
+    cudaFree(b->d_flags);
+    if (b->h_flags)
+        cudaFreeHost(b->h_flags);
+    delete b;
+}
+
+static int batch_graph(FcabBatch *b, int steps)
+{
+    if (b->graph && b->graph_steps == steps)
+        return 0;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g;
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess)
+        return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+    cudaError_t le = cudaSuccess;
+    for (int i = 0; i < steps && le == cudaSuccess; i++)
+        le = b->L.step(b->d_members, b->d_unit_member, b->total_units, b->d_q, b->grid,
+                       b->stream);
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || e != cudaSuccess)
+        return bfail(FCAB_ERR_CUDA, "fcab_batch: graph capture failed");
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+        return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+    b->graph_steps = steps;
+    return 0;
+}
+
+extern "C" int fcab_batch_run(FcabBatch *b, double window_s, int graph_steps, int max_windows)
+{
+    const bool paced = window_s > 0.0;
+    const int steps = graph_steps > 0 ? graph_steps : 16;
+    int rc = batch_graph(b, steps);
+    if (rc)
+        return rc;
+    cudaError_t e;
+    int opened = 0;
+    if (paced) {
+        e = b->L.window(b->d_members, b->n, window_s, b->stream);
+        if (e != cudaSuccess)
+            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+        b->launches += 1;
+        b->windows += 1;
+        opened = 1;
+    }
+    for (;;) {
+        e = cudaGraphLaunch(b->graph, b->stream);
+        if (e != cudaSuccess)
+            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+        b->launches += steps;
+        b->replays += 1;
+        k_gather_active<<<(b->n + 127) / 128, 128, 0, b->stream>>>(b->d_members, b->n,
+                                                                   b->d_flags);
+        b->launches += 1;
+        e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * b->n, cudaMemcpyDeviceToHost,
+                            b->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess)
+            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+        int running = 0, paused = 0;
+        for (int i = 0; i < b->n; i++) {
+            running += b->h_flags[i] == 1;
+            paused += b->h_flags[i] == 2;
+        }
+        if (running)
+            continue;
+        if (!paused || !paced || (max_windows > 0 && opened >= max_windows))
+            break;
+        e = b->L.window(b->d_members, b->n, window_s, b->stream);
+        if (e != cudaSuccess)
+            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+        b->launches += 1;
+        b->windows += 1;
+        opened += 1;
+    }
+    return 0;
+}
+
+extern "C" int fcab_batch_info(FcabBatch *b, FcabBatchInfo *info)
+{
+    info->members = b->n;
+    info->cols_per_lane = b->key.cpl;
+    info->seg_rows = b->seg;
+    info->grid = b->grid;
+    info->total_units = b->total_units;
+    info->launches = b->launches;
+    info->windows = b->windows;
+    info->graph_replays = b->replays;
+    return 0;
+}

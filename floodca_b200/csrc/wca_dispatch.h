@@ -27,6 +27,32 @@ struct Launchers {
     const void *step_fn;   // __global__ symbol, for occupancy queries
 };
 
+// Batched-ensemble launchers (FP32 state, FP64 accumulation).
+struct BatchLaunchers {
+    cudaError_t (*step)(const void *members, const int *unit_member, int total_units, BatchQ *q,
+                        int grid, cudaStream_t s);
+    cudaError_t (*window)(const void *members, int n, double window, cudaStream_t s);
+    const void *step_fn;
+};
+bool lookup_batch_f32(const VariantKey &k, BatchLaunchers *out);
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LAND>
+cudaError_t launch_batch(const void *members, const int *unit_member, int total_units, BatchQ *q,
+                         int grid, cudaStream_t s)
+{
+    k_step_batch<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, 128, 0, s>>>(
+        static_cast<const MemberD<T> *>(members), unit_member, total_units, q);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_window(const void *members, int n, double window, cudaStream_t s)
+{
+    k_batch_window<T><<<(n + 127) / 128, 128, 0, s>>>(static_cast<const MemberD<T> *>(members),
+                                                       n, window);
+    return cudaGetLastError();
+}
+
 // Returns false when the variant is not compiled.
 bool lookup_f32(const VariantKey &k, Launchers *out);
 bool lookup_f32all(const VariantKey &k, Launchers *out);

@@ -79,6 +79,7 @@ struct Ctl {
     unsigned long long vmax_bits;
     unsigned int ctas_done;
     unsigned int launches;
+    double window_end;          // > 0: pause once t reaches it (batched ensembles)
     double V_in;                // inflow volume added by the steps taken
     double V_in_step;           // inflow volume of the prepared step
     double accd[4][NSLOT];      // V_rain, clamp, V_sea, V_bnd (double accumulation)
@@ -208,6 +209,8 @@ __device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool afte
     }
     if (!done && after_step && tc.progress_every > 0 && step % tc.progress_every == 0)
         pause = 1;
+    if (!done && c->window_end > 0.0 && t >= c->window_end - 1e-9)
+        pause = 1;                  // end of an output window
     T dt_base = (T)c->dt_base;
     if (!done && step % tc.U == 0) {
         T vmax;
@@ -460,522 +463,549 @@ __device__ __forceinline__ AccT acc_mul(T a, T x)
         return (float)(a * x);
 }
 
-// LANDONLY: every cell of the grid is LAND; the mask is not read and the
-// padding around the grid carries z = PAD_Z (> any terrain), h = 0, which
-// makes every face to it carry zero discharge (hf = max(L) - max(z) = 0).
-template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
-                                              int warps_total)
+// Per-step values every warp of a step reads (from the control block).
+template <typename T>
+struct StepVals {
+    StepK<T> k;
+    T dt, A, F, tmax_val, inflow_dh, rainv, dd, qnan;
+    int want_v;
+    const T *hin;
+    T *hout;
+};
+
+template <typename T, int K>
+__device__ __forceinline__ StepVals<T> step_vals(const GridD<T> &g, const RunK<T> &rk,
+                                                const Ctl *ctl)
 {
-    using G = Geom<CPL>;
-    if (ctl->active == 0)
-        return;
-    const int lane = threadIdx.x & 31;
-    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    StepVals<T> v;
+    v.k = rk.k;
+    v.k.dt = (T)ctl->dt;
+    v.k.den = (T)(2 * K) * v.k.dt;
+    v.k.rden = T(1) / v.k.den;
+    v.dt = v.k.dt;
+    v.A = v.k.A;
+    v.F = (T)ctl->F;
+    v.tmax_val = (T)ctl->tmax_val;
+    v.inflow_dh = (T)ctl->inflow_dh;
+    v.want_v = ctl->want_v;
+    v.hin = ctl->h_cur ? g.h1 : g.h0;
+    v.hout = ctl->h_cur ? g.h0 : g.h1;
+    v.rainv = rk.cr_uniform * v.F;   // C*Rday*F for a uniform field
+    v.dd = v.k.d_diag;
+    v.qnan = qnan_of<T>();
+    return v;
+}
 
-    StepK<T> k = rk.k;
-    k.dt = (T)ctl->dt;
-    k.den = (T)(2 * K) * k.dt;
-    k.rden = T(1) / k.den;
-    const T dt = k.dt, A = k.A;
-    const T F = (T)ctl->F;
-    const T tmax_val = (T)ctl->tmax_val;
-    const T inflow_dh = (T)ctl->inflow_dh;
-    const int want_v = ctl->want_v;
-    const T *hin = ctl->h_cur ? g.h1 : g.h0;
-    T *hout = ctl->h_cur ? g.h0 : g.h1;
-    const T rainv = rk.cr_uniform * F;   // C*Rday*F for a uniform field
-    const T dd = k.d_diag;
-    const T qnan = qnan_of<T>();
-
+// A warp's running sums over the cells it writes.
+template <typename T, typename AccT>
+struct StepSums {
     AccT a_rain = 0, a_clamp = 0, a_sea = 0, a_bnd = 0;
     double rain_sum = 0.0;       // sum of rain depths (per-cell rain field)
     long long rain_cells = 0;    // LAND output cells (uniform rain)
     unsigned capn = 0;
     T vmax = T(0);
+};
 
+// One warp streams output rows [r0, r1) of one strip through the pipeline.
+// LANDONLY: every cell of the grid is LAND; the mask is not read and the
+// padding around the grid carries z = PAD_Z (> any terrain), h = 0, which
+// makes every face to it carry zero discharge (hf = max(L) - max(z) = 0).
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
+__device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &rk,
+                                              const StepVals<T> &sv, int strip, int r0, int r1,
+                                              int lane, StepSums<T, AccT> &ss)
+{
+    using G = Geom<CPL>;
+    const StepK<T> &k = sv.k;
+    const T dt = sv.dt, A = sv.A, F = sv.F, tmax_val = sv.tmax_val, inflow_dh = sv.inflow_dh;
+    const T rainv = sv.rainv, dd = sv.dd, qnan = sv.qnan;
+    const int want_v = sv.want_v;
+    const T *hin = sv.hin;
+    T *hout = sv.hout;
     const int nr = g.nr, nc = g.nc;
-    const int nstrips = (nc + G::OW - 1) / G::OW;
-    const long long total = (long long)nstrips * nr;
-    long long w0 = total * wid / warps_total, w1 = total * (wid + 1) / warps_total;
-    if (wid >= warps_total)
-        w0 = w1 = 0;
+    AccT &a_clamp = ss.a_clamp, &a_sea = ss.a_sea, &a_bnd = ss.a_bnd, &a_rain = ss.a_rain;
+    double &rain_sum = ss.rain_sum;
+    long long &rain_cells = ss.rain_cells;
+    unsigned &capn = ss.capn;
+    T &vmax = ss.vmax;
+    (void)a_rain;
+    (void)rain_sum;
 
-    while (w0 < w1) {
-        const int strip = (int)(w0 / nr);
-        const int r0 = (int)(w0 % nr);
-        const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
-        w0 += r1 - r0;
-
-        const int cbase = strip * G::OW - G::HL + lane * CPL;   // first column of the lane
-        const bool out_lane = lane * CPL >= G::HL && lane * CPL < G::HL + G::OW;
-        const long long colo = (long long)(cbase + PADC);
-        // columns of this lane inside the grid (padding columns are WALL in the
-        // generic layout, but LAND-like in the LANDONLY layout)
-        bool colok[CPL];
+    const int cbase = strip * G::OW - G::HL + lane * CPL;   // first column of the lane
+    const bool out_lane = lane * CPL >= G::HL && lane * CPL < G::HL + G::OW;
+    const long long colo = (long long)(cbase + PADC);
+    // columns of this lane inside the grid (padding columns are WALL in the
+    // generic layout, but LAND-like in the LANDONLY layout)
+    bool colok[CPL];
 #pragma unroll
-        for (int j = 0; j < CPL; j++)
-            colok[j] = !LANDONLY || (cbase + j >= 0 && cbase + j < nc);
-        // does this lane hold column 0 or column nc-1 (open-edge candidates)?
-        const bool edge_lane = (cbase <= 0 && cbase + CPL > 0) || (cbase <= nc - 1 && cbase + CPL > nc - 1);
+    for (int j = 0; j < CPL; j++)
+        colok[j] = !LANDONLY || (cbase + j >= 0 && cbase + j < nc);
+    // does this lane hold column 0 or column nc-1 (open-edge candidates)?
+    const bool edge_lane = (cbase <= 0 && cbase + CPL > 0) || (cbase <= nc - 1 && cbase + CPL > nc - 1);
 
-        // Pipeline registers; the comments give the rows they hold while
-        // iteration i runs stages C..E (face rows are the upper cell's row).
-        Row<T, CPL> nx, cu, p1, p2, p3;      // rows i+1, i, i-1, i-2, i-3
-        T X1[CPL], X2[CPL];                  // x-faces of rows i-1, i-2
-        T Y1[CPL], Y2[CPL];                  // y-faces of rows i-2, i-3
-        T E1[CPL], E2[CPL];                  // K=8 SE faces of rows i-2, i-3
-        T W1[CPL], W2[CPL];                  // K=8 SW faces of rows i-2, i-3
-        T s1[CPL], s2[CPL];                  // limiter of rows i-2, i-3
-        T qo1[CPL];                          // open-edge discharge of row i-2
-        int ko1[CPL];                        // open sides of row i-2
-        T L3[CPL], L4[CPL];                  // new level (NaN: WALL) of rows i-3, i-4
-        T hn3[CPL];                          // new depth of row i-3
-        unsigned eflag = 0u;                 // stage-E candidates of row i-3 (bit per column)
-        T hm[CPL];                           // hmax of row i-2
-        T cr1[CPL];                          // rain field of row i-2
+    // Pipeline registers; the comments give the rows they hold while
+    // iteration i runs stages C..E (face rows are the upper cell's row).
+    Row<T, CPL> nx, cu, p1, p2, p3;      // rows i+1, i, i-1, i-2, i-3
+    T X1[CPL], X2[CPL];                  // x-faces of rows i-1, i-2
+    T Y1[CPL], Y2[CPL];                  // y-faces of rows i-2, i-3
+    T E1[CPL], E2[CPL];                  // K=8 SE faces of rows i-2, i-3
+    T W1[CPL], W2[CPL];                  // K=8 SW faces of rows i-2, i-3
+    T s1[CPL], s2[CPL];                  // limiter of rows i-2, i-3
+    T qo1[CPL];                          // open-edge discharge of row i-2
+    int ko1[CPL];                        // open sides of row i-2
+    T L3[CPL], L4[CPL];                  // new level (NaN: WALL) of rows i-3, i-4
+    T hn3[CPL];                          // new depth of row i-3
+    unsigned eflag = 0u;                 // stage-E candidates of row i-3 (bit per column)
+    T hm[CPL];                           // hmax of row i-2
+    T cr1[CPL];                          // rain field of row i-2
 #pragma unroll
-        for (int j = 0; j < CPL; j++) {
-            X1[j] = X2[j] = Y1[j] = Y2[j] = T(0);
-            E1[j] = E2[j] = W1[j] = W2[j] = T(0);
-            s1[j] = s2[j] = T(1);
-            qo1[j] = T(0);
-            ko1[j] = 0;
-            L3[j] = L4[j] = qnan;
-            hn3[j] = T(0);
-            hm[j] = T(0);
-            cr1[j] = T(0);
-            cu.z[j] = cu.h[j] = cu.n[j] = T(0);
-            cu.m[j] = M_WALL;
-        }
+    for (int j = 0; j < CPL; j++) {
+        X1[j] = X2[j] = Y1[j] = Y2[j] = T(0);
+        E1[j] = E2[j] = W1[j] = W2[j] = T(0);
+        s1[j] = s2[j] = T(1);
+        qo1[j] = T(0);
+        ko1[j] = 0;
+        L3[j] = L4[j] = qnan;
+        hn3[j] = T(0);
+        hm[j] = T(0);
+        cr1[j] = T(0);
+        cu.z[j] = cu.h[j] = cu.n[j] = T(0);
+        cu.m[j] = M_WALL;
+    }
+    p1 = cu;
+    p2 = cu;
+    p3 = cu;
+    load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(r0 - 3 + PADR) * g.pitch + colo);
+
+    for (int i = r0 - 3; i <= r1 + 2; i++) {
+        p3 = p2;
+        p2 = p1;
         p1 = cu;
-        p2 = cu;
-        p3 = cu;
-        load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(r0 - 3 + PADR) * g.pitch + colo);
+        cu = nx;
+        load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(i + 1 + PADR) * g.pitch + colo);
+        const bool row0_out = i >= r0 && i < r1;
+        const bool row1_out = i - 1 >= r0 && i - 1 < r1;
+        const bool row2_out = i - 2 >= r0 && i - 2 < r1;
+        // hmax and rain field of row i-1, used by stage D next iteration
+        const long long off1 = (long long)(i - 1 + PADR) * g.pitch + colo;
+        T hm_next[CPL], cr_next[CPL];
+        if (row1_out && out_lane)
+            VecIO<T, CPL>::ld_rw(hm_next, g.hmax + off1);
+        if constexpr (RAINF)
+            VecIO<T, CPL>::ld(cr_next, g.cr + off1);
 
-        for (int i = r0 - 3; i <= r1 + 2; i++) {
-            p3 = p2;
-            p2 = p1;
-            p1 = cu;
-            cu = nx;
-            load_row<T, CPL, LANDONLY>(nx, g, hin, (long long)(i + 1 + PADR) * g.pitch + colo);
-            const bool row0_out = i >= r0 && i < r1;
-            const bool row1_out = i - 1 >= r0 && i - 1 < r1;
-            const bool row2_out = i - 2 >= r0 && i - 2 < r1;
-            // hmax and rain field of row i-1, used by stage D next iteration
-            const long long off1 = (long long)(i - 1 + PADR) * g.pitch + colo;
-            T hm_next[CPL], cr_next[CPL];
-            if (row1_out && out_lane)
-                VecIO<T, CPL>::ld_rw(hm_next, g.hmax + off1);
-            if constexpr (RAINF)
-                VecIO<T, CPL>::ld(cr_next, g.cr + off1);
-
-            // ---- A: x-faces of row i; y and diagonal faces of row i-1,
-            //      all evaluated together (faces_q) for instruction-level
-            //      parallelism across the NF independent faces
-            T X0[CPL], Yn[CPL], En[CPL], Wn[CPL];
-            {
-                constexpr int NF = (K == 8 ? 4 : 2) * CPL;
-                const T cz = sh_dn(cu.z[0]), ch = sh_dn(cu.h[0]), cn = sh_dn(cu.n[0]);
-                const uint32_t cm = LANDONLY ? (uint32_t)M_LAND : sh_dn(cu.m[0]);
-                T pz = T(0), ph = T(0), pn = T(0);
-                uint32_t pm = M_LAND;
-                if constexpr (K == 8) {
-                    pz = sh_dn(p1.z[0]);
-                    ph = sh_dn(p1.h[0]);
-                    pn = sh_dn(p1.n[0]);
-                    if constexpr (!LANDONLY)
-                        pm = sh_dn(p1.m[0]);
-                }
-                T fza[NF], fha[NF], fna[NF], fzb[NF], fhb[NF], fnb[NF], fd[NF], frd[NF];
-                uint32_t fma_[NF], fmb[NF];
-#pragma unroll
-                for (int j = 0; j < CPL; j++) {
-                    const T zr = right_of<T, CPL>(cu.z, j, cz), hr = right_of<T, CPL>(cu.h, j, ch);
-                    const T nrr = right_of<T, CPL>(cu.n, j, cn);
-                    const uint32_t mr = right_of<uint32_t, CPL>(cu.m, j, cm);
-                    // x-face (i, c) -> (i, c+1)
-                    fza[j] = cu.z[j]; fha[j] = cu.h[j]; fna[j] = cu.n[j]; fma_[j] = cu.m[j];
-                    fzb[j] = zr; fhb[j] = hr; fnb[j] = nrr; fmb[j] = mr;
-                    fd[j] = k.dx; frd[j] = k.rdx;
-                    // y-face (i-1, c) -> (i, c)
-                    const int y = CPL + j;
-                    fza[y] = p1.z[j]; fha[y] = p1.h[j]; fna[y] = p1.n[j]; fma_[y] = p1.m[j];
-                    fzb[y] = cu.z[j]; fhb[y] = cu.h[j]; fnb[y] = cu.n[j]; fmb[y] = cu.m[j];
-                    fd[y] = k.dx; frd[y] = k.rdx;
-                    if constexpr (K == 8) {
-                        // SE face (i-1, c) -> (i, c+1)
-                        const int e = 2 * CPL + j;
-                        fza[e] = p1.z[j]; fha[e] = p1.h[j]; fna[e] = p1.n[j]; fma_[e] = p1.m[j];
-                        fzb[e] = zr; fhb[e] = hr; fnb[e] = nrr; fmb[e] = mr;
-                        fd[e] = dd; frd[e] = k.rdd;
-                        // SW face (i-1, c+1) -> (i, c)
-                        const int w = 3 * CPL + j;
-                        fza[w] = right_of<T, CPL>(p1.z, j, pz);
-                        fha[w] = right_of<T, CPL>(p1.h, j, ph);
-                        fna[w] = right_of<T, CPL>(p1.n, j, pn);
-                        fma_[w] = right_of<uint32_t, CPL>(p1.m, j, pm);
-                        fzb[w] = cu.z[j]; fhb[w] = cu.h[j]; fnb[w] = cu.n[j]; fmb[w] = cu.m[j];
-                        fd[w] = dd; frd[w] = k.rdd;
-                    }
-                }
-                T fq[NF];
-                unsigned fc[NF];
-                faces_q<T, MATH, LANDONLY, NF>(fza, fha, fna, fma_, fzb, fhb, fnb, fmb, fd, frd, k,
-                                               fq, fc);
-                unsigned c0 = 0u, c1 = 0u;
-#pragma unroll
-                for (int j = 0; j < CPL; j++) {
-                    X0[j] = fq[j];
-                    Yn[j] = fq[CPL + j];
-                    c0 += fc[j];
-                    c1 += fc[CPL + j];
-                    if constexpr (K == 8) {
-                        En[j] = fq[2 * CPL + j];
-                        Wn[j] = fq[3 * CPL + j];
-                        c1 += fc[2 * CPL + j] + fc[3 * CPL + j];
-                    } else {
-                        En[j] = Wn[j] = T(0);
-                    }
-                }
-                if (out_lane) {
-                    if (row0_out)
-                        capn += c0;
-                    if (row1_out)
-                        capn += c1;
-                }
+        // ---- A: x-faces of row i; y and diagonal faces of row i-1,
+        //      all evaluated together (faces_q) for instruction-level
+        //      parallelism across the NF independent faces
+        T X0[CPL], Yn[CPL], En[CPL], Wn[CPL];
+        {
+            constexpr int NF = (K == 8 ? 4 : 2) * CPL;
+            const T cz = sh_dn(cu.z[0]), ch = sh_dn(cu.h[0]), cn = sh_dn(cu.n[0]);
+            const uint32_t cm = LANDONLY ? (uint32_t)M_LAND : sh_dn(cu.m[0]);
+            T pz = T(0), ph = T(0), pn = T(0);
+            uint32_t pm = M_LAND;
+            if constexpr (K == 8) {
+                pz = sh_dn(p1.z[0]);
+                ph = sh_dn(p1.h[0]);
+                pn = sh_dn(p1.n[0]);
+                if constexpr (!LANDONLY)
+                    pm = sh_dn(p1.m[0]);
             }
-
-            // ---- C: outflow and limiter of row i-1, in the reference face
-            //      order +x, -x, +y, -y, [d1+, d1-, d2+, d2-], open slots
-            T s0[CPL], qo0[CPL];
-            int ko0[CPL];
-            {
-                const T xl = sh_up(X1[CPL - 1]);
-                T el = T(0), wl = T(0);
-                if constexpr (K == 8) {
-                    el = sh_up(E1[CPL - 1]);
-                    wl = sh_up(Wn[CPL - 1]);
-                }
-                const int r = i - 1;
-                const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
-#pragma unroll
-                for (int j = 0; j < CPL; j++) {
-                    const int c = cbase + j;
-                    int kop = 0;
-                    if ((edge_row || edge_lane) && rk.open && p1.m[j] == M_LAND)
-                        kop = (c == 0 && rk.edge_w) + (c == nc - 1 && rk.edge_e) +
-                              (r == 0 && rk.edge_n) + (r == nr - 1 && rk.edge_s);
-                    T qo = T(0);
-                    if (kop) {
-                        int cap;
-                        qo = open_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], k, cap);
-                        if (row1_out && out_lane)
-                            capn += (unsigned)(cap * kop);
-                    }
-                    qo0[j] = qo;
-                    ko0[j] = kop;
-                    // positive outgoing parts in the reference order; adding a
-                    // zero leaves a non-negative sum unchanged
-                    T out = T(0);
-                    out += fmax(X1[j], T(0));
-                    out += fmax(-left_of<T, CPL>(X1, j, xl), T(0));
-                    out += fmax(Yn[j], T(0));
-                    out += fmax(-Y1[j], T(0));
-                    if constexpr (K == 8) {
-                        out += fmax(En[j], T(0));
-                        out += fmax(-left_of<T, CPL>(E1, j, el), T(0));
-                        out += fmax(left_of<T, CPL>(Wn, j, wl), T(0));
-                        out += fmax(-W1[j], T(0));
-                    }
-                    out += open_sum<T>(qo, kop);
-                    const T ov = out * dt;
-                    s0[j] = p1.m[j] == M_LAND ? limiter_bf<T, MATH>(ov, p1.h[j], A) : T(1);
-                }
-            }
-
-            unsigned eflag_next = 0u;
-            // ---- D: limiter-scaled net inflow and depth update of row i-2
-            //      (s0: row i-1 below, s1: the row itself, s2: row i-3 above)
-            T hn2[CPL], Ln2[CPL];
-            {
-                const int r = i - 2;
-                const T sl = sh_up(s1[CPL - 1]), sr = sh_dn(s1[0]);
-                const T xl = sh_up(X2[CPL - 1]);
-                T bl = T(1), br = T(1), al = T(1), ar = T(1), el = T(0), wl = T(0);
-                if constexpr (K == 8) {
-                    bl = sh_up(s0[CPL - 1]);
-                    br = sh_dn(s0[0]);
-                    al = sh_up(s2[CPL - 1]);
-                    ar = sh_dn(s2[0]);
-                    el = sh_up(E2[CPL - 1]);
-                    wl = sh_up(W1[CPL - 1]);
-                }
-                uint32_t ml = 0, mr = 0, m1l = 0, m1r = 0, m3l = 0, m3r = 0;
-                if (rk.has_sea) {
-                    ml = sh_up(p2.m[CPL - 1]);
-                    mr = sh_dn(p2.m[0]);
-                    if constexpr (K == 8) {
-                        m1l = sh_up(p1.m[CPL - 1]);
-                        m1r = sh_dn(p1.m[0]);
-                        m3l = sh_up(p3.m[CPL - 1]);
-                        m3r = sh_dn(p3.m[0]);
-                    }
-                }
-                const bool sea_on = rk.has_sea != 0;
-                const bool inflow_row = r == rk.inflow_r;
-                // open-edge terms exist only on open edge rows or edge lanes
-                const bool open2 = edge_lane || (rk.open && ((r == 0 && rk.edge_n) ||
-                                                             (r == nr - 1 && rk.edge_s)));
-                const bool row2_in = r >= 0 && r < nr;
-                // stage-E threshold: the warp's running velocity maximum
-                const T thr = want_v ? warp_max_nonneg(vmax) : T(0);
-                T *tm_row = g.tmax + (long long)(r + PADR) * g.pitch + colo;
-                bool rose_any = false, bnd_open = false;
-                T qbnd[CPL];
-                if constexpr (LANDONLY && sizeof(AccT) == 8 && !RAINF) {
-                    if (row2_out && out_lane) {
-#pragma unroll
-                        for (int j = 0; j < CPL; j++)
-                            rain_cells += colok[j] ? 1 : 0;
-                    }
-                }
-                T hmx[CPL];
-#pragma unroll
-                for (int j = 0; j < CPL; j++) {
-                    const uint32_t ma = p2.m[j];
-                    const bool land = ma == M_LAND;
-                    const T sa = s1[j];
-                    T net = T(0), Q, Qs;
-                    double sea = 0.0;
-                    // +x: face (r, c) -> (r, c+1)
-                    Q = X2[j];
-                    Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s1, j, sr));
-                    net -= Qs;
-                    if (sea_on && land && right_of<uint32_t, CPL>(p2.m, j, mr) == M_SEA && Qs > T(0))
-                        sea += (double)dt * (double)Qs;
-                    // -x: face (r, c-1) -> (r, c)
-                    Q = left_of<T, CPL>(X2, j, xl);
-                    Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s1, j, sl) : sa);
-                    net += Qs;
-                    if (sea_on && land && left_of<uint32_t, CPL>(p2.m, j, ml) == M_SEA && Qs < T(0))
-                        sea += (double)dt * (double)(-Qs);
-                    // +y: face (r, c) -> (r+1, c)
-                    Q = Y1[j];
-                    Qs = Q * (Q >= T(0) ? sa : s0[j]);
-                    net -= Qs;
-                    if (sea_on && land && p1.m[j] == M_SEA && Qs > T(0))
-                        sea += (double)dt * (double)Qs;
-                    // -y: face (r-1, c) -> (r, c)
-                    Q = Y2[j];
-                    Qs = Q * (Q >= T(0) ? s2[j] : sa);
-                    net += Qs;
-                    if (sea_on && land && p3.m[j] == M_SEA && Qs < T(0))
-                        sea += (double)dt * (double)(-Qs);
-                    if constexpr (K == 8) {
-                        // d1+: (r, c) -> (r+1, c+1)
-                        Q = E1[j];
-                        Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s0, j, br));
-                        net -= Qs;
-                        if (sea_on && land && right_of<uint32_t, CPL>(p1.m, j, m1r) == M_SEA &&
-                            Qs > T(0))
-                            sea += (double)dt * (double)Qs;
-                        // d1-: (r-1, c-1) -> (r, c)
-                        Q = left_of<T, CPL>(E2, j, el);
-                        Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s2, j, al) : sa);
-                        net += Qs;
-                        if (sea_on && land && left_of<uint32_t, CPL>(p3.m, j, m3l) == M_SEA &&
-                            Qs < T(0))
-                            sea += (double)dt * (double)(-Qs);
-                        // d2+: (r, c) -> (r+1, c-1), SW face of index (r, c-1)
-                        Q = left_of<T, CPL>(W1, j, wl);
-                        Qs = Q * (Q >= T(0) ? sa : left_of<T, CPL>(s0, j, bl));
-                        net -= Qs;
-                        if (sea_on && land && left_of<uint32_t, CPL>(p1.m, j, m1l) == M_SEA &&
-                            Qs > T(0))
-                            sea += (double)dt * (double)Qs;
-                        // d2-: (r-1, c+1) -> (r, c), SW face of index (r-1, c)
-                        Q = W2[j];
-                        Qs = Q * (Q >= T(0) ? right_of<T, CPL>(s2, j, ar) : sa);
-                        net += Qs;
-                        if (sea_on && land && right_of<uint32_t, CPL>(p3.m, j, m3r) == M_SEA &&
-                            Qs < T(0))
-                            sea += (double)dt * (double)(-Qs);
-                    }
-                    T Qo = T(0);
-                    if (open2) {
-                        Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
-                        net -= Qo;
-                    }
-                    const bool cell_out = row2_out && out_lane && colok[j];
-                    T ha = p2.h[j];
-                    const T rain = RAINF ? cr1[j] * F : rainv;
-                    T hu = ha + (dt * Mth<T, MATH>::div_c(net, A, k.inv_A) + rain);
-                    hu = land ? hu : ha;
-                    // rare events are settled after the loop: clamp, open edge, sea
-                    if (land && hu < T(0)) {
-                        if (cell_out)
-                            a_clamp += acc_mul<AccT, T>(-hu, A);
-                        hu = T(0);
-                    }
-                    ha = hu;
-                    if (inflow_row && land && cbase + j == rk.inflow_c)
-                        ha = ha + inflow_dh;
-                    if constexpr (sizeof(AccT) == 4) {
-                        if (cell_out && land)
-                            a_rain += A * rain;
-                    } else if constexpr (RAINF) {
-                        rain_sum += (cell_out && land) ? (double)rain : 0.0;
-                    } else if constexpr (!LANDONLY) {
-                        rain_cells += (cell_out && land) ? 1 : 0;
-                    }
-                    if (sea_on && cell_out)
-                        a_sea += (AccT)sea;
-                    if (open2)
-                        bnd_open |= cell_out && ko1[j] != 0;
-                    qbnd[j] = Qo;
-                    if constexpr (LANDONLY) {
-                        // outside the grid: keep the padding depth, no face
-                        const bool inside = colok[j] && row2_in;
-                        hn2[j] = inside ? ha : p2.h[j];
-                        Ln2[j] = inside ? p2.z[j] + ha : qnan;
-                    } else {
-                        hn2[j] = ha;
-                        Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
-                    }
-                    if (want_v && cell_out && land && ha >= k.tau_h &&
-                        !(thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, ha)))
-                        eflag_next |= 1u << j;
-                    const bool rise = cell_out && land && ha > hm[j];
-                    hmx[j] = rise ? ha : hm[j];
-                    rose_any |= rise;
-                    if (rise)
-                        tm_row[j] = tmax_val;
-                }
-                if (bnd_open) {
-#pragma unroll
-                    for (int j = 0; j < CPL; j++)
-                        if (row2_out && out_lane && colok[j] && ko1[j])
-                            a_bnd += acc_mul<AccT, T>(dt, qbnd[j]);
-                }
-                if (row2_out && out_lane) {
-                    const long long off2 = (long long)(r + PADR) * g.pitch + colo;
-                    VecIO<T, CPL>::st(hout + off2, hn2);
-                    if (rose_any)
-                        VecIO<T, CPL>::st(g.hmax + off2, hmx);
-                }
-            }
-
-            // ---- E: next step's stable velocity of row i-3 from the new
-            //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2), for the
-            //      cells stage D flagged: wet LAND output cells whose critical
-            //      velocity could exceed the warp's running maximum (every
-            //      other cell's velocity is capped below it).
-            if (want_v && __any_sync(0xffffffffu, eflag != 0u)) {
-                const int r = i - 3;
-                vmax = warp_max_nonneg(vmax);
-                const T Ll = sh_up(L3[CPL - 1]), Lr = sh_dn(L3[0]);
-                T L2l = T(0), L2r = T(0), L4l = T(0), L4r = T(0);
-                if constexpr (K == 8) {
-                    L2l = sh_up(Ln2[CPL - 1]);
-                    L2r = sh_dn(Ln2[0]);
-                    L4l = sh_up(L4[CPL - 1]);
-                    L4r = sh_dn(L4[0]);
-                }
-                const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
-#pragma unroll
-                for (int j = 0; j < CPL; j++) {
-                    if (!(eflag & (1u << j)))
-                        continue;
-                    const T hv = hn3[j];
-                    const int c = cbase + j;
-                    const T la = L3[j];
-                    T mo = T(0);
-                    mo = fmax(mo, fabs(la - right_of<T, CPL>(L3, j, Lr)));
-                    mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
-                    mo = fmax(mo, fabs(la - Ln2[j]));
-                    mo = fmax(mo, fabs(la - L4[j]));
-                    if (edge_row || (edge_lane && rk.open &&
-                                     ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e)))) {
-                        const T lv = p3.z[j] - k.S_bnd * k.dx;
-                        mo = fmax(mo, fabs(la - lv));
-                    }
-                    T md = T(0);
-                    if constexpr (K == 8) {
-                        md = fmax(md, fabs(la - right_of<T, CPL>(Ln2, j, L2r)));
-                        md = fmax(md, fabs(la - left_of<T, CPL>(Ln2, j, L2l)));
-                        md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
-                        md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
-                    }
-                    // cheap upper bound first; the exact velocity only when
-                    // it could raise the running maximum
-                    T Sb = mo * k.rdx;
-                    if constexpr (K == 8) {
-                        const T sd = md * k.rdd;
-                        Sb = sd > Sb ? sd : Sb;
-                    }
-                    if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <= vmax)
-                        continue;
-                    T Smax = Mth<T, MATH>::div(mo, k.dx);
-                    if constexpr (K == 8) {
-                        const T Sd = Mth<T, MATH>::div(md, dd);
-                        if (Sd > Smax)
-                            Smax = Sd;
-                    }
-                    const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
-                    if (v > vmax)
-                        vmax = v;
-                }
-            }
-
-            // ---- advance the pipeline
+            T fza[NF], fha[NF], fna[NF], fzb[NF], fhb[NF], fnb[NF], fd[NF], frd[NF];
+            uint32_t fma_[NF], fmb[NF];
 #pragma unroll
             for (int j = 0; j < CPL; j++) {
-                X2[j] = X1[j];
-                X1[j] = X0[j];
-                Y2[j] = Y1[j];
-                Y1[j] = Yn[j];
+                const T zr = right_of<T, CPL>(cu.z, j, cz), hr = right_of<T, CPL>(cu.h, j, ch);
+                const T nrr = right_of<T, CPL>(cu.n, j, cn);
+                const uint32_t mr = right_of<uint32_t, CPL>(cu.m, j, cm);
+                // x-face (i, c) -> (i, c+1)
+                fza[j] = cu.z[j]; fha[j] = cu.h[j]; fna[j] = cu.n[j]; fma_[j] = cu.m[j];
+                fzb[j] = zr; fhb[j] = hr; fnb[j] = nrr; fmb[j] = mr;
+                fd[j] = k.dx; frd[j] = k.rdx;
+                // y-face (i-1, c) -> (i, c)
+                const int y = CPL + j;
+                fza[y] = p1.z[j]; fha[y] = p1.h[j]; fna[y] = p1.n[j]; fma_[y] = p1.m[j];
+                fzb[y] = cu.z[j]; fhb[y] = cu.h[j]; fnb[y] = cu.n[j]; fmb[y] = cu.m[j];
+                fd[y] = k.dx; frd[y] = k.rdx;
                 if constexpr (K == 8) {
-                    E2[j] = E1[j];
-                    E1[j] = En[j];
-                    W2[j] = W1[j];
-                    W1[j] = Wn[j];
+                    // SE face (i-1, c) -> (i, c+1)
+                    const int e = 2 * CPL + j;
+                    fza[e] = p1.z[j]; fha[e] = p1.h[j]; fna[e] = p1.n[j]; fma_[e] = p1.m[j];
+                    fzb[e] = zr; fhb[e] = hr; fnb[e] = nrr; fmb[e] = mr;
+                    fd[e] = dd; frd[e] = k.rdd;
+                    // SW face (i-1, c+1) -> (i, c)
+                    const int w = 3 * CPL + j;
+                    fza[w] = right_of<T, CPL>(p1.z, j, pz);
+                    fha[w] = right_of<T, CPL>(p1.h, j, ph);
+                    fna[w] = right_of<T, CPL>(p1.n, j, pn);
+                    fma_[w] = right_of<uint32_t, CPL>(p1.m, j, pm);
+                    fzb[w] = cu.z[j]; fhb[w] = cu.h[j]; fnb[w] = cu.n[j]; fmb[w] = cu.m[j];
+                    fd[w] = dd; frd[w] = k.rdd;
                 }
-                s2[j] = s1[j];
-                s1[j] = s0[j];
-                qo1[j] = qo0[j];
-                ko1[j] = ko0[j];
-                L4[j] = L3[j];
-                L3[j] = Ln2[j];
-                hn3[j] = hn2[j];
-                eflag = eflag_next;
-                if (row1_out && out_lane)
-                    hm[j] = hm_next[j];
-                if constexpr (RAINF)
-                    cr1[j] = cr_next[j];
+            }
+            T fq[NF];
+            unsigned fc[NF];
+            faces_q<T, MATH, LANDONLY, NF>(fza, fha, fna, fma_, fzb, fhb, fnb, fmb, fd, frd, k,
+                                           fq, fc);
+            unsigned c0 = 0u, c1 = 0u;
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                X0[j] = fq[j];
+                Yn[j] = fq[CPL + j];
+                c0 += fc[j];
+                c1 += fc[CPL + j];
+                if constexpr (K == 8) {
+                    En[j] = fq[2 * CPL + j];
+                    Wn[j] = fq[3 * CPL + j];
+                    c1 += fc[2 * CPL + j] + fc[3 * CPL + j];
+                } else {
+                    En[j] = Wn[j] = T(0);
+                }
+            }
+            if (out_lane) {
+                if (row0_out)
+                    capn += c0;
+                if (row1_out)
+                    capn += c1;
             }
         }
-    }
 
-    // ---- publish the warp's accumulators and velocity maximum
+        // ---- C: outflow and limiter of row i-1, in the reference face
+        //      order +x, -x, +y, -y, [d1+, d1-, d2+, d2-], open slots
+        T s0[CPL], qo0[CPL];
+        int ko0[CPL];
+        {
+            const T xl = sh_up(X1[CPL - 1]);
+            T el = T(0), wl = T(0);
+            if constexpr (K == 8) {
+                el = sh_up(E1[CPL - 1]);
+                wl = sh_up(Wn[CPL - 1]);
+            }
+            const int r = i - 1;
+            const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                const int c = cbase + j;
+                int kop = 0;
+                if ((edge_row || edge_lane) && rk.open && p1.m[j] == M_LAND)
+                    kop = (c == 0 && rk.edge_w) + (c == nc - 1 && rk.edge_e) +
+                          (r == 0 && rk.edge_n) + (r == nr - 1 && rk.edge_s);
+                T qo = T(0);
+                if (kop) {
+                    int cap;
+                    qo = open_q<T, MATH>(p1.z[j], p1.h[j], p1.n[j], p1.m[j], k, cap);
+                    if (row1_out && out_lane)
+                        capn += (unsigned)(cap * kop);
+                }
+                qo0[j] = qo;
+                ko0[j] = kop;
+                // positive outgoing parts in the reference order; adding a
+                // zero leaves a non-negative sum unchanged
+                T out = T(0);
+                out += fmax(X1[j], T(0));
+                out += fmax(-left_of<T, CPL>(X1, j, xl), T(0));
+                out += fmax(Yn[j], T(0));
+                out += fmax(-Y1[j], T(0));
+                if constexpr (K == 8) {
+                    out += fmax(En[j], T(0));
+                    out += fmax(-left_of<T, CPL>(E1, j, el), T(0));
+                    out += fmax(left_of<T, CPL>(Wn, j, wl), T(0));
+                    out += fmax(-W1[j], T(0));
+                }
+                out += open_sum<T>(qo, kop);
+                const T ov = out * dt;
+                s0[j] = p1.m[j] == M_LAND ? limiter_bf<T, MATH>(ov, p1.h[j], A) : T(1);
+            }
+        }
+
+        unsigned eflag_next = 0u;
+        // ---- D: limiter-scaled net inflow and depth update of row i-2
+        //      (s0: row i-1 below, s1: the row itself, s2: row i-3 above)
+        T hn2[CPL], Ln2[CPL];
+        {
+            const int r = i - 2;
+            const T sl = sh_up(s1[CPL - 1]), sr = sh_dn(s1[0]);
+            const T xl = sh_up(X2[CPL - 1]);
+            T bl = T(1), br = T(1), al = T(1), ar = T(1), el = T(0), wl = T(0);
+            if constexpr (K == 8) {
+                bl = sh_up(s0[CPL - 1]);
+                br = sh_dn(s0[0]);
+                al = sh_up(s2[CPL - 1]);
+                ar = sh_dn(s2[0]);
+                el = sh_up(E2[CPL - 1]);
+                wl = sh_up(W1[CPL - 1]);
+            }
+            uint32_t ml = 0, mr = 0, m1l = 0, m1r = 0, m3l = 0, m3r = 0;
+            if (rk.has_sea) {
+                ml = sh_up(p2.m[CPL - 1]);
+                mr = sh_dn(p2.m[0]);
+                if constexpr (K == 8) {
+                    m1l = sh_up(p1.m[CPL - 1]);
+                    m1r = sh_dn(p1.m[0]);
+                    m3l = sh_up(p3.m[CPL - 1]);
+                    m3r = sh_dn(p3.m[0]);
+                }
+            }
+            const bool sea_on = rk.has_sea != 0;
+            const bool inflow_row = r == rk.inflow_r;
+            // open-edge terms exist only on open edge rows or edge lanes
+            const bool open2 = edge_lane || (rk.open && ((r == 0 && rk.edge_n) ||
+                                                         (r == nr - 1 && rk.edge_s)));
+            const bool row2_in = r >= 0 && r < nr;
+            // stage-E threshold: the warp's running velocity maximum
+            const T thr = want_v ? warp_max_nonneg(vmax) : T(0);
+            T *tm_row = g.tmax + (long long)(r + PADR) * g.pitch + colo;
+            bool rose_any = false, bnd_open = false;
+            T qbnd[CPL];
+            if constexpr (LANDONLY && sizeof(AccT) == 8 && !RAINF) {
+                if (row2_out && out_lane) {
+#pragma unroll
+                    for (int j = 0; j < CPL; j++)
+                        rain_cells += colok[j] ? 1 : 0;
+                }
+            }
+            T hmx[CPL];
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                const uint32_t ma = p2.m[j];
+                const bool land = ma == M_LAND;
+                const T sa = s1[j];
+                T net = T(0), Q, Qs;
+                double sea = 0.0;
+                // +x: face (r, c) -> (r, c+1)
+                Q = X2[j];
+                Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s1, j, sr));
+                net -= Qs;
+                if (sea_on && land && right_of<uint32_t, CPL>(p2.m, j, mr) == M_SEA && Qs > T(0))
+                    sea += (double)dt * (double)Qs;
+                // -x: face (r, c-1) -> (r, c)
+                Q = left_of<T, CPL>(X2, j, xl);
+                Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s1, j, sl) : sa);
+                net += Qs;
+                if (sea_on && land && left_of<uint32_t, CPL>(p2.m, j, ml) == M_SEA && Qs < T(0))
+                    sea += (double)dt * (double)(-Qs);
+                // +y: face (r, c) -> (r+1, c)
+                Q = Y1[j];
+                Qs = Q * (Q >= T(0) ? sa : s0[j]);
+                net -= Qs;
+                if (sea_on && land && p1.m[j] == M_SEA && Qs > T(0))
+                    sea += (double)dt * (double)Qs;
+                // -y: face (r-1, c) -> (r, c)
+                Q = Y2[j];
+                Qs = Q * (Q >= T(0) ? s2[j] : sa);
+                net += Qs;
+                if (sea_on && land && p3.m[j] == M_SEA && Qs < T(0))
+                    sea += (double)dt * (double)(-Qs);
+                if constexpr (K == 8) {
+                    // d1+: (r, c) -> (r+1, c+1)
+                    Q = E1[j];
+                    Qs = Q * (Q >= T(0) ? sa : right_of<T, CPL>(s0, j, br));
+                    net -= Qs;
+                    if (sea_on && land && right_of<uint32_t, CPL>(p1.m, j, m1r) == M_SEA &&
+                        Qs > T(0))
+                        sea += (double)dt * (double)Qs;
+                    // d1-: (r-1, c-1) -> (r, c)
+                    Q = left_of<T, CPL>(E2, j, el);
+                    Qs = Q * (Q >= T(0) ? left_of<T, CPL>(s2, j, al) : sa);
+                    net += Qs;
+                    if (sea_on && land && left_of<uint32_t, CPL>(p3.m, j, m3l) == M_SEA &&
+                        Qs < T(0))
+                        sea += (double)dt * (double)(-Qs);
+                    // d2+: (r, c) -> (r+1, c-1), SW face of index (r, c-1)
+                    Q = left_of<T, CPL>(W1, j, wl);
+                    Qs = Q * (Q >= T(0) ? sa : left_of<T, CPL>(s0, j, bl));
+                    net -= Qs;
+                    if (sea_on && land && left_of<uint32_t, CPL>(p1.m, j, m1l) == M_SEA &&
+                        Qs > T(0))
+                        sea += (double)dt * (double)Qs;
+                    // d2-: (r-1, c+1) -> (r, c), SW face of index (r-1, c)
+                    Q = W2[j];
+                    Qs = Q * (Q >= T(0) ? right_of<T, CPL>(s2, j, ar) : sa);
+                    net += Qs;
+                    if (sea_on && land && right_of<uint32_t, CPL>(p3.m, j, m3r) == M_SEA &&
+                        Qs < T(0))
+                        sea += (double)dt * (double)(-Qs);
+                }
+                T Qo = T(0);
+                if (open2) {
+                    Qo = open_sum<T>(qo1[j] * sa, ko1[j]);
+                    net -= Qo;
+                }
+                const bool cell_out = row2_out && out_lane && colok[j];
+                T ha = p2.h[j];
+                const T rain = RAINF ? cr1[j] * F : rainv;
+                T hu = ha + (dt * Mth<T, MATH>::div_c(net, A, k.inv_A) + rain);
+                hu = land ? hu : ha;
+                // rare events are settled after the loop: clamp, open edge, sea
+                if (land && hu < T(0)) {
+                    if (cell_out)
+                        a_clamp += acc_mul<AccT, T>(-hu, A);
+                    hu = T(0);
+                }
+                ha = hu;
+                if (inflow_row && land && cbase + j == rk.inflow_c)
+                    ha = ha + inflow_dh;
+                if constexpr (sizeof(AccT) == 4) {
+                    if (cell_out && land)
+                        a_rain += A * rain;
+                } else if constexpr (RAINF) {
+                    rain_sum += (cell_out && land) ? (double)rain : 0.0;
+                } else if constexpr (!LANDONLY) {
+                    rain_cells += (cell_out && land) ? 1 : 0;
+                }
+                if (sea_on && cell_out)
+                    a_sea += (AccT)sea;
+                if (open2)
+                    bnd_open |= cell_out && ko1[j] != 0;
+                qbnd[j] = Qo;
+                if constexpr (LANDONLY) {
+                    // outside the grid: keep the padding depth, no face
+                    const bool inside = colok[j] && row2_in;
+                    hn2[j] = inside ? ha : p2.h[j];
+                    Ln2[j] = inside ? p2.z[j] + ha : qnan;
+                } else {
+                    hn2[j] = ha;
+                    Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
+                }
+                if (want_v && cell_out && land && ha >= k.tau_h &&
+                    !(thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, ha)))
+                    eflag_next |= 1u << j;
+                const bool rise = cell_out && land && ha > hm[j];
+                hmx[j] = rise ? ha : hm[j];
+                rose_any |= rise;
+                if (rise)
+                    tm_row[j] = tmax_val;
+            }
+            if (bnd_open) {
+#pragma unroll
+                for (int j = 0; j < CPL; j++)
+                    if (row2_out && out_lane && colok[j] && ko1[j])
+                        a_bnd += acc_mul<AccT, T>(dt, qbnd[j]);
+            }
+            if (row2_out && out_lane) {
+                const long long off2 = (long long)(r + PADR) * g.pitch + colo;
+                VecIO<T, CPL>::st(hout + off2, hn2);
+                if (rose_any)
+                    VecIO<T, CPL>::st(g.hmax + off2, hmx);
+            }
+        }
+
+        // ---- E: next step's stable velocity of row i-3 from the new
+        //      levels of rows i-4 (L4), i-3 (L3) and i-2 (Ln2), for the
+        //      cells stage D flagged: wet LAND output cells whose critical
+        //      velocity could exceed the warp's running maximum (every
+        //      other cell's velocity is capped below it).
+        if (want_v && __any_sync(0xffffffffu, eflag != 0u)) {
+            const int r = i - 3;
+            vmax = warp_max_nonneg(vmax);
+            const T Ll = sh_up(L3[CPL - 1]), Lr = sh_dn(L3[0]);
+            T L2l = T(0), L2r = T(0), L4l = T(0), L4r = T(0);
+            if constexpr (K == 8) {
+                L2l = sh_up(Ln2[CPL - 1]);
+                L2r = sh_dn(Ln2[0]);
+                L4l = sh_up(L4[CPL - 1]);
+                L4r = sh_dn(L4[0]);
+            }
+            const bool edge_row = rk.open && ((r == 0 && rk.edge_n) || (r == nr - 1 && rk.edge_s));
+#pragma unroll
+            for (int j = 0; j < CPL; j++) {
+                if (!(eflag & (1u << j)))
+                    continue;
+                const T hv = hn3[j];
+                const int c = cbase + j;
+                const T la = L3[j];
+                T mo = T(0);
+                mo = fmax(mo, fabs(la - right_of<T, CPL>(L3, j, Lr)));
+                mo = fmax(mo, fabs(la - left_of<T, CPL>(L3, j, Ll)));
+                mo = fmax(mo, fabs(la - Ln2[j]));
+                mo = fmax(mo, fabs(la - L4[j]));
+                if (edge_row || (edge_lane && rk.open &&
+                                 ((c == 0 && rk.edge_w) || (c == nc - 1 && rk.edge_e)))) {
+                    const T lv = p3.z[j] - k.S_bnd * k.dx;
+                    mo = fmax(mo, fabs(la - lv));
+                }
+                T md = T(0);
+                if constexpr (K == 8) {
+                    md = fmax(md, fabs(la - right_of<T, CPL>(Ln2, j, L2r)));
+                    md = fmax(md, fabs(la - left_of<T, CPL>(Ln2, j, L2l)));
+                    md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
+                    md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
+                }
+                // cheap upper bound first; the exact velocity only when
+                // it could raise the running maximum
+                T Sb = mo * k.rdx;
+                if constexpr (K == 8) {
+                    const T sd = md * k.rdd;
+                    Sb = sd > Sb ? sd : Sb;
+                }
+                if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <= vmax)
+                    continue;
+                T Smax = Mth<T, MATH>::div(mo, k.dx);
+                if constexpr (K == 8) {
+                    const T Sd = Mth<T, MATH>::div(md, dd);
+                    if (Sd > Smax)
+                        Smax = Sd;
+                }
+                const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
+                if (v > vmax)
+                    vmax = v;
+            }
+        }
+
+        // ---- advance the pipeline
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            X2[j] = X1[j];
+            X1[j] = X0[j];
+            Y2[j] = Y1[j];
+            Y1[j] = Yn[j];
+            if constexpr (K == 8) {
+                E2[j] = E1[j];
+                E1[j] = En[j];
+                W2[j] = W1[j];
+                W1[j] = Wn[j];
+            }
+            s2[j] = s1[j];
+            s1[j] = s0[j];
+            qo1[j] = qo0[j];
+            ko1[j] = ko0[j];
+            L4[j] = L3[j];
+            L3[j] = Ln2[j];
+            hn3[j] = hn2[j];
+            eflag = eflag_next;
+            if (row1_out && out_lane)
+                hm[j] = hm_next[j];
+            if constexpr (RAINF)
+                cr1[j] = cr_next[j];
+        }
+    }
+}
+
+// Publishes a warp's sums to a control block: accumulator slot `slot`,
+// velocity maximum for the next dt.
+template <typename T, typename AccT, bool RAINF>
+__device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVals<T> &sv,
+                                             Ctl *ctl, int lane, int slot)
+{
+    AccT a_rain = ss.a_rain;
     if constexpr (sizeof(AccT) == 8) {
         if constexpr (RAINF)
-            a_rain = (double)A * rain_sum;
+            a_rain = (double)sv.A * ss.rain_sum;
         else
-            a_rain = (double)rain_cells * ((double)A * (double)rainv);
+            a_rain = (double)ss.rain_cells * ((double)sv.A * (double)sv.rainv);
     }
     a_rain = warp_sum(a_rain);
-    a_clamp = warp_sum(a_clamp);
-    a_sea = warp_sum(a_sea);
-    a_bnd = warp_sum(a_bnd);
-    capn = warp_sum(capn);
+    const AccT a_clamp = warp_sum(ss.a_clamp);
+    const AccT a_sea = warp_sum(ss.a_sea);
+    const AccT a_bnd = warp_sum(ss.a_bnd);
+    const unsigned capn = warp_sum(ss.capn);
+    T vmax = ss.vmax;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const T vo = __shfl_xor_sync(0xffffffffu, vmax, o);
         vmax = vo > vmax ? vo : vmax;
     }
     if (lane == 0) {
-        const int slot = wid & (NSLOT - 1);
         if constexpr (sizeof(AccT) == 8) {
             if (a_rain != 0) atomicAdd(&ctl->accd[0][slot], (double)a_rain);
             if (a_clamp != 0) atomicAdd(&ctl->accd[1][slot], (double)a_clamp);
@@ -989,13 +1019,43 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
         }
         if (capn)
             atomicAdd(&ctl->cap[slot], (unsigned long long)capn);
-        if (want_v && vmax > T(0)) {
+        if (sv.want_v && vmax > T(0)) {
             if constexpr (sizeof(T) == 4)
                 atomicMax(&ctl->vmax_bits, (unsigned long long)__float_as_uint((float)vmax));
             else
                 atomicMax(&ctl->vmax_bits, (unsigned long long)__double_as_longlong((double)vmax));
         }
     }
+}
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
+__global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
+                                              int warps_total)
+{
+    using G = Geom<CPL>;
+    if (ctl->active == 0)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const StepVals<T> sv = step_vals<T, K>(g, rk, ctl);
+    StepSums<T, AccT> ss;
+
+    const int nr = g.nr, nc = g.nc;
+    const int nstrips = (nc + G::OW - 1) / G::OW;
+    const long long total = (long long)nstrips * nr;
+    long long w0 = total * wid / warps_total, w1 = total * (wid + 1) / warps_total;
+    if (wid >= warps_total)
+        w0 = w1 = 0;
+
+    while (w0 < w1) {
+        const int strip = (int)(w0 / nr);
+        const int r0 = (int)(w0 % nr);
+        const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
+        w0 += r1 - r0;
+        sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
+    }
+
+    publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, wid & (NSLOT - 1));
     // ---- the last CTA to finish prepares the next step
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1007,6 +1067,97 @@ __global__ void __launch_bounds__(128) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc
             ctl->launches += 1;
             finalize<T>(ctl, tc, rk, true);
         }
+    }
+}
+
+// --------------------------------------------------------------------------
+// Batched step: one launch advances every active member of an ensemble by
+// one step. Members keep their own grids, control blocks, dt and time. Warps
+// take work units (member, row block, strip) from an atomic queue; a unit of
+// an inactive member (finished, or paused at its window end) is skipped. The
+// warp that completes a member's last unit prepares that member's next step.
+// The last warp to leave resets the queue for the next launch. No warp ever
+// waits for another.
+
+template <typename T>
+struct MemberD {
+    GridD<T> g;
+    RunK<T> rk;
+    TimeCfg tc;
+    Ctl *ctl;
+    int unit_off, units, strips, seg;
+};
+
+struct BatchQ {
+    unsigned int next_unit;
+    unsigned int warps_out;
+};
+
+template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
+__global__ void __launch_bounds__(128, CPL == 2 ? 3 : 1)
+k_step_batch(const MemberD<T> *members,
+                                                    const int *unit_member, int total_units,
+                                                    BatchQ *q)
+{
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned u = 0;
+        if (lane == 0)
+            u = atomicAdd(&q->next_unit, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= (unsigned)total_units)
+            break;
+        const int m = unit_member[u];
+        const MemberD<T> &md = members[m];
+        Ctl *ctl = md.ctl;
+        if (ctl->active == 0)
+            continue;
+        const GridD<T> g = md.g;
+        const RunK<T> rk = md.rk;
+        const int local = (int)u - md.unit_off;
+        const int strip = local % md.strips, blk = local / md.strips;
+        const int r0 = blk * md.seg, r1 = min(g.nr, r0 + md.seg);
+        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl);
+        StepSums<T, AccT> ss;
+        sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
+        publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, (int)(u & (NSLOT - 1)));
+        if (lane == 0) {
+            __threadfence();
+            const unsigned prev = atomicAdd(&ctl->ctas_done, 1u);
+            if (prev == (unsigned)md.units - 1u) {
+                __threadfence();
+                ctl->h_cur ^= 1;
+                ctl->launches += 1;
+                const TimeCfg tc = md.tc;
+                finalize<T>(ctl, tc, rk, true);
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        __threadfence();
+        const unsigned nw = gridDim.x * (blockDim.x >> 5);
+        if (atomicAdd(&q->warps_out, 1u) == nw - 1u) {
+            q->next_unit = 0u;
+            q->warps_out = 0u;
+        }
+    }
+}
+
+// Opens the next output window of every member that is not finished.
+template <typename T>
+__global__ void k_batch_window(const MemberD<T> *members, int n, double window)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n)
+        return;
+    Ctl *c = members[m].ctl;
+    if (c->done)
+        return;
+    c->window_end += window;
+    if (c->pause && c->t < c->window_end - 1e-9) {
+        c->pause = 0;
+        c->active = 1;
     }
 }
 

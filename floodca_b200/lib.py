@@ -10,7 +10,7 @@ import ctypes as C
 from functools import lru_cache
 from pathlib import Path
 
-from .abi import FcabConfig, FcabInfo, FcabPoll, FcabStats, fca_types
+from .abi import FcabBatchInfo, FcabConfig, FcabInfo, FcabPoll, FcabStats, fca_types
 
 PKG = Path(__file__).resolve().parent
 LIB_CORE = PKG / "libfloodca_b200_core.so"
@@ -62,6 +62,11 @@ def core() -> C.CDLL:
         "fcab_sim_stream": (_P, [_P]),
         "fcab_sim_destroy": (None, [_P]),
         "fcab_math_probe": (C.c_int, [C.c_int, _P, _P, _P, C.c_longlong, C.c_float]),
+        "fcab_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int,
+                                        C.c_int, C.c_int, C.POINTER(C.c_int), _P]),
+        "fcab_batch_run": (C.c_int, [_P, C.c_double, C.c_int, C.c_int]),
+        "fcab_batch_info": (C.c_int, [_P, C.POINTER(FcabBatchInfo)]),
+        "fcab_batch_destroy": (None, [_P]),
         "fcab_run_noalloc": (C.c_int, [C.POINTER(FcabConfig), _P, _P, _P, _P, _P, _P, _P, _P,
                                        _P, C.POINTER(FcabStats)]),
         "fcab_last_error": (C.c_char_p, []),

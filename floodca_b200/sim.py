@@ -82,8 +82,9 @@ class RunParams:
         return replace(self, **kw)
 
 
-def make_config(dom: Domain, p: RunParams, precision="f32", math="exact", cols_per_lane=0,
+def make_config(dom, p: RunParams, precision="f32", math="exact", cols_per_lane=0,
                 seg_rows=0) -> FcabConfig:
+    """dom: a Domain, or anything with .shape (rows, cols) and .dx."""
     c = FcabConfig()
     core().fcab_config_defaults(C.byref(c), dom.shape[0], dom.shape[1])
     c.precision, c.math = PREC[precision], MATH[math]
@@ -119,19 +120,41 @@ class Session:
 
     def __init__(self, dom: Domain, p: RunParams, precision: str = "f32", math: str = "exact",
                  cols_per_lane: int = 0, seg_rows: int = 0, stream=None):
+        self.dom = dom.astype(np.float64 if precision == "f64" else np.float32)
+        self._create(self.dom, p, precision, math, cols_per_lane, seg_rows, stream)
+        d = self.dom
+        R = effective_rday(d, p, self.dtype)
+        check(self.L.fcab_sim_upload(self.h, _ptr(d.z), _ptr(d.h), _ptr(d.n), _ptr(d.C), _ptr(R),
+                                     _ptr(d.mask), _ptr(d.hmax), _ptr(d.tmax)), "fcab_sim_upload")
+
+    def _create(self, dom, p, precision, math, cols_per_lane, seg_rows, stream):
         self.L = core()
         self.precision = precision
         self.dtype = np.float64 if precision == "f64" else np.float32
-        self.dom = dom.astype(self.dtype)
+        self.shape = tuple(dom.shape)
         self.p = p
-        self.cfg = make_config(self.dom, p, precision, math, cols_per_lane, seg_rows)
+        self.cfg = make_config(dom, p, precision, math, cols_per_lane, seg_rows)
         h = C.c_void_p()
         check(self.L.fcab_sim_create(C.byref(h), C.byref(self.cfg), stream), "fcab_sim_create")
         self.h = h
-        d = self.dom
-        R = effective_rday(d, p, self.dtype)
-        check(self.L.fcab_sim_upload(h, _ptr(d.z), _ptr(d.h), _ptr(d.n), _ptr(d.C), _ptr(R),
-                                     _ptr(d.mask), _ptr(d.hmax), _ptr(d.tmax)), "fcab_sim_upload")
+
+    @classmethod
+    def from_device(cls, shape, dx: float, p: RunParams, z, h, mask, n=None, Cf=None,
+                    Rday=None, precision: str = "f32", math: str = "exact",
+                    cols_per_lane: int = 0, seg_rows: int = 0, stream=None) -> "Session":
+        """A session uploaded from device arrays (row-major, contiguous, of the
+        precision's element type; mask uint8), given as raw pointers or as
+        objects with data_ptr(). Rday is used as given (lambda already applied)."""
+        from types import SimpleNamespace
+        s = cls.__new__(cls)
+        s.dom = None
+        s._create(SimpleNamespace(shape=tuple(shape), dx=dx), p, precision, math,
+                  cols_per_lane, seg_rows, stream)
+        ptr = lambda a: None if a is None else C.c_void_p(a.data_ptr() if hasattr(a, "data_ptr")
+                                                           else int(a))
+        check(s.L.fcab_sim_upload_device(s.h, ptr(z), ptr(h), ptr(n), ptr(Cf), ptr(Rday),
+                                         ptr(mask), None, None), "fcab_sim_upload_device")
+        return s
 
     # -- running -------------------------------------------------------------
     def advance(self, nsteps: int) -> None:
@@ -157,7 +180,7 @@ class Session:
         return {f[0]: getattr(i, f[0]) for f in i._fields_}
 
     def download(self):
-        nr, nc = self.dom.shape
+        nr, nc = self.shape
         h = np.empty((nr, nc), self.dtype)
         hmax = np.empty((nr, nc), self.dtype)
         tmax = np.empty((nr, nc), self.dtype)

@@ -281,6 +281,42 @@ FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uin
 /* The session's cudaStream_t. */
 FCAB_API void *fcab_sim_stream(FcabSim *s);
 
+/* ---- Batched ensembles (no reference counterpart; the reference runs
+ * members one at a time, src/hybrid/main_ens_mpi_cuda.c:69-120). ---- */
+typedef struct FcabBatch FcabBatch;
+
+typedef struct FcabBatchInfo {
+    int members, cols_per_lane, seg_rows, grid, total_units;
+    long long launches, windows, graph_replays;
+} FcabBatchInfo;
+
+/* Groups uploaded sessions into one batch. Members must share FP32
+ * precision, K, math mode, rain form (uniform or field), mask form and
+ * device; sizes, parameters, rain and time differ freely. cols_per_lane
+ * (1, 2, 4; 0 = 2) sets the strip width of every member; a member's work
+ * units are strips of member_seg_rows[i] rows (NULL: seg_rows for every
+ * member; values <= 0 mean 64). stream: cudaStream_t or NULL (the first
+ * member's). */
+FCAB_API int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n,
+                               int cols_per_lane, int seg_rows, const int *member_seg_rows,
+                               void *stream);
+
+/* Runs every member to the end of its run. One launch advances every active
+ * member by one step, in graphs of graph_steps launches. window_s > 0 paces
+ * the members by output windows: replays continue until every member reaches
+ * the end of the current window (window_s seconds of simulated time past the
+ * previous one; steps land on window ends when out_every divides window_s),
+ * then the next window opens; max_windows > 0 stops after that many windows.
+ * window_s <= 0 runs every member freely to its end. Pacing never changes a
+ * member's steps: they are those of its own session run alone. Members with
+ * forcing days or progress pauses are refused at fcab_batch_create. Member
+ * results are read with fcab_sim_stats / fcab_sim_download. */
+FCAB_API int fcab_batch_run(FcabBatch *b, double window_s, int graph_steps, int max_windows);
+
+FCAB_API int fcab_batch_info(FcabBatch *b, FcabBatchInfo *info);
+
+FCAB_API void fcab_batch_destroy(FcabBatch *b);
+
 /* Runs cfg->max_steps steps of the FP32 WCA step (the same fused kernel as
  * the sessions) on caller-owned device arrays, allocating nothing. No
  * counterpart in the reference. For callers that cannot call cudaMalloc:

@@ -340,6 +340,8 @@ def main(argv=None) -> int:
     ap.add_argument("--math", default="exact")
     ap.add_argument("--hours", type=float, default=8.0)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tuning-cache", default=str(TUNING_FILE))
+    ap.add_argument("--retune", action="store_true")
     ap.add_argument("--paced", action="store_true", help="also time the 10-minute paced run")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
@@ -353,7 +355,9 @@ def main(argv=None) -> int:
         dist.init_process_group("nccl")
     mine = shard(members, rank, world)
     local = [members[i] for i in mine]
-    tune = DEFAULT_TUNING if a.no_tune else autotune(members, a.math)
+    tune = DEFAULT_TUNING if a.no_tune else autotune(members, a.math,
+                                                     cache=Path(a.tuning_cache),
+                                                     force=a.retune)
     bat = run_batched(local, a.math, tune, window=0.0)
     wall = bat["wall_s"]
     if world > 1:

@@ -29,6 +29,8 @@ def _load(path: Path) -> C.CDLL:
 
 
 _P = C.c_void_p
+_I = C.c_int
+_LL = C.c_longlong
 
 
 @lru_cache(maxsize=1)
@@ -69,6 +71,26 @@ def core() -> C.CDLL:
         "fcab_batch_destroy": (None, [_P]),
         "fcab_run_noalloc": (C.c_int, [C.POINTER(FcabConfig), _P, _P, _P, _P, _P, _P, _P, _P,
                                        _P, C.POINTER(FcabStats)]),
+        # surrogate layers
+        "fcab_unet_conv_fwd": (C.c_int, [_P, _I, _I, _I, _I, _P, _I, _P, _I, _P, _P]),
+        "fcab_unet_conv_dgrad": (C.c_int, [_P, _I, _I, _I, _I, _P, _I, _P, _P]),
+        "fcab_unet_conv_wgrad": (C.c_int, [_P, _P, _I, _I, _I, _I, _I, _P, _P]),
+        "fcab_unet_maxpool2": (C.c_int, [_P, _P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_maxpool2_bwd": (C.c_int, [_P, _P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_upsample2": (C.c_int, [_P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_upsample2_bwd": (C.c_int, [_P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_concat": (C.c_int, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_add": (C.c_int, [_P, _P, _LL, _P]),
+        "fcab_unet_relu_bwd": (C.c_int, [_P, _P, _LL, _P]),
+        "fcab_unet_dropout": (C.c_int, [_P, _LL, C.c_float, C.c_uint32, _P]),
+        "fcab_unet_bias_grad": (C.c_int, [_P, _LL, _I, _P, _P]),
+        "fcab_unet_head_fwd": (C.c_int, [_P, _P, _P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_head_bwd": (C.c_int, [_P] * 8 + [_I, _I, _I, _I, _P]),
+        "fcab_unet_prep_weights": (C.c_int, [_P, _P, _P, _I, _I, _P]),
+        "fcab_unet_adam": (C.c_int, [_P, _P, _P, _P, _LL, C.c_float, C.c_float, C.c_float,
+                                     C.c_float, _I, C.c_float, _P]),
+        "fcab_unet_pack_input": (C.c_int, [_P, _I, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_device_error": (C.c_int, []),
         "fcab_last_error": (C.c_char_p, []),
         "fcab_version": (C.c_char_p, []),
     }

@@ -369,6 +369,66 @@ FCAB_API const char *fcab_last_error(void);
 /* Library build identification (e.g. "floodca_b200 sm_100a"). */
 FCAB_API const char *fcab_version(void);
 
+/* ---- Flood-depth surrogate layers (no reference counterpart: FloodCA has
+ * no surrogate). Activations are bf16 matrices [N*(H+2)*(W+2)][C] of NHWC
+ * images with a one-pixel zero border (C a multiple of 16); kernels write
+ * interior pixels only, so borders stay zero once the buffer is zeroed.
+ * Weights are [Cout][9][Cin] bf16 (tap = ky*3 + kx). All calls are
+ * asynchronous on `stream` (cudaStream_t or NULL) and return 0 or an
+ * FCAB_ERR_* code with fcab_last_error(). ---- */
+
+/* y = conv3x3(x, w) (+ bias[Cout] fp32, ReLU when relu != 0). Cin % 16 == 0,
+ * Cout % 32 == 0. tcgen05 tensor cores, FP32 accumulation. */
+FCAB_API int fcab_unet_conv_fwd(const void *x, int N, int H, int W, int Cin, const void *w,
+                                int Cout, const float *bias, int relu, void *y, void *stream);
+/* dx[.][Cin] = data gradient of the convolution given dy[.][Cout] and the
+ * flipped, transposed weights wt[Cin][9][Cout] (fcab_unet_prep_weights). */
+FCAB_API int fcab_unet_conv_dgrad(const void *dy, int N, int H, int W, int Cout, const void *wt,
+                                  int Cin, void *dx, void *stream);
+/* dw[Cout][9][Cin] (fp32) += weight gradient from dy[.][Cout] and x[.][Cin]. */
+FCAB_API int fcab_unet_conv_wgrad(const void *dy, const void *x, int N, int H, int W, int Cin,
+                                  int Cout, float *dw, void *stream);
+/* 2x2 max pooling of an (H, W) image; idx[N][H/2][W/2][C] records the arg max. */
+FCAB_API int fcab_unet_maxpool2(const void *x, void *y, uint8_t *idx, int N, int H, int W, int C,
+                                void *stream);
+FCAB_API int fcab_unet_maxpool2_bwd(const void *dy, const uint8_t *idx, void *dx, int N, int H,
+                                    int W, int C, void *stream);
+/* Nearest 2x upsampling of an (H, W) image; the backward sums 2x2 children. */
+FCAB_API int fcab_unet_upsample2(const void *x, void *y, int N, int H, int W, int C, void *stream);
+FCAB_API int fcab_unet_upsample2_bwd(const void *dy, void *dx, int N, int H, int W, int C,
+                                     void *stream);
+/* y = [a | b] along channels (backward != 0: split y into a and b). */
+FCAB_API int fcab_unet_concat(const void *a, int Ca, const void *b, int Cb, void *y, int N, int H,
+                              int W, int backward, void *stream);
+/* y += x, n bf16 elements. */
+FCAB_API int fcab_unet_add(void *y, const void *x, long long n, void *stream);
+/* g *= (y > 0), n elements. */
+FCAB_API int fcab_unet_relu_bwd(void *g, const void *y, long long n, void *stream);
+/* In-place inverted dropout with a hashed mask of (seed, element). */
+FCAB_API int fcab_unet_dropout(void *x, long long n, float p, uint32_t seed, void *stream);
+/* db[c] += sum over the P rows of g[.][C]. */
+FCAB_API int fcab_unet_bias_grad(const void *g, long long P, int C, float *db, void *stream);
+/* 1x1 output head C -> 1: out[N][H][W] fp32. */
+FCAB_API int fcab_unet_head_fwd(const void *x, const float *w, const float *b, float *out, int N,
+                                int H, int W, int C, void *stream);
+/* Mean squared error of out against target: dx (bf16), dw, db, loss sum
+ * (accumulated). */
+FCAB_API int fcab_unet_head_bwd(const void *x, const float *w, const float *out,
+                                const float *target, void *dx, float *dw, float *db, float *loss,
+                                int N, int H, int W, int C, void *stream);
+/* fp32 master weights -> bf16 forward weights wb and dgrad weights wt. */
+FCAB_API int fcab_unet_prep_weights(const float *w, void *wb, void *wt, int Cout, int Cin,
+                                    void *stream);
+/* Adam step t (>= 1) with decoupled-free L2 term wd. */
+FCAB_API int fcab_unet_adam(float *w, const float *g, float *m, float *v, long long n, float lr,
+                            float b1, float b2, float eps, int t, float wd, void *stream);
+/* fp32 [N][H][W][Cs] -> bf16 bordered matrix with C >= Cs channels. */
+FCAB_API int fcab_unet_pack_input(const float *in, int Cs, void *x, int C, int N, int H, int W,
+                                  void *stream);
+/* Returns and clears the device-side error code of these kernels (0: none;
+ * nonzero: a pipeline wait gave up). */
+FCAB_API int fcab_unet_device_error(void);
+
 #ifdef __cplusplus
 }
 #endif

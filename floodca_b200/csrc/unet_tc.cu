@@ -173,137 +173,273 @@ __device__ __forceinline__ bool interior(int p, int P, int Hp, int Wp)
 }
 
 // ---------------------------------------------------------------------------
-// Implicit-GEMM 3x3 convolution: M = 128 pixels per CTA, N = BN output
-// channels, K = 9 taps x Cin in chunks of CK channels.
-// Warp 0 lane 0 issues TMA loads, warp 1 lane 0 issues MMAs; all four warps
-// run the epilogue (TMEM lane quarter of warp w = tile rows 32w..32w+31).
+// Implicit-GEMM 3x3 convolution, persistent and warp-specialised: each CTA
+// (one per SM) walks tiles of M = 128 pixels x N = BN output channels;
+// K = 9 taps x Cin in blocks of CK channels.
+//   warp 0      TMA producer (A blocks into a ring of up to 32 stages; the weights
+//               either per block or, when small, once into resident smem)
+//   warp 1      MMA issuer (one thread), accumulating into one of two TMEM
+//               buffers so the epilogue of a tile overlaps the next tile
+//   warps 2-9   epilogue, two warpgroups, one per TMEM buffer (tiles of
+//               even / odd local index): TMEM -> bias, ReLU -> bf16 rows
+//               of interior pixels (warp w reads TMEM lanes 32*(w%4)..+31)
 
 struct GemmArgs {
-    int P, Hp, Wp;     // padded pixel count, padded height and width
-    int Cin;           // channels of the A matrix
-    int Cout;          // channels (row width) of the output matrix
-    const float *bias; // [Cout] or null
-    bf16 *y;           // [P][Cout]
+    int P, Hp, Wp;          // padded pixel count, padded height and width
+    int Cin;                // channels of the A matrix
+    int Cout;               // channels (row width) of the output matrix
+    int mtiles, ntiles;     // pixel tiles, total tiles (pixel tiles x channel tiles)
+    int nkb;                // K blocks per tile (9 * Cin / CK)
+    int bres;               // 1: the weights stay resident in shared memory
+    int stages;             // A (or A+B) ring stages
+    int stage_bytes;        // bytes per stage (multiple of 1024)
+    unsigned long long m_hw, m_w;   // ceil(2^48 / (Hp*Wp)), ceil(2^48 / Wp)
+    const float *bias;      // [Cout] or null
+    bf16 *y;                // [P][Cout]
     int relu;
 };
 
+// A stage holds G taps of one channel block (G = 1, 3 or 9 for 64-, 32- and
+// 16-channel blocks), so one barrier round trip covers at least 64 K of MMAs.
 template <int CK, int BN>
 struct GemmCfg {
-    static constexpr int A_BYTES = 128 * CK * 2;
+    static constexpr int G = CK == 64 ? 1 : CK == 32 ? 3 : 9;
+    static constexpr int A_BYTES = 128 * CK * 2;          // one tap
     static constexpr int B_BYTES = BN * CK * 2;
-    static constexpr int TX_BYTES = A_BYTES + B_BYTES;              // bytes of the two boxes
-    static constexpr int STAGE = (TX_BYTES + 1023) / 1024 * 1024;   // 1024-aligned stage stride
-    static constexpr int STAGES = (196608 / STAGE) < 8 ? (196608 / STAGE) : 8;
+    static constexpr int B_AL = (B_BYTES + 1023) / 1024 * 1024;
     static constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
-    static constexpr int SMEM = 1024 + STAGES * STAGE + (2 * STAGES + 1) * 8 + 16;
 };
 
+// Descriptor of a K-major tile at shared address saddr (LBO 16 B).
+template <int CK>
+__device__ __forceinline__ uint64_t kdesc(uint32_t saddr)
+{
+    constexpr uint64_t hi = ((uint64_t)((KSw<CK>::sbo >> 4) & 0x3FFFu)) | (1ull << 14) |
+                            ((uint64_t)KSw<CK>::layout << 29);
+    return (hi << 32) | (uint64_t)(((saddr & 0x3FFFFu) >> 4) | (1u << 16));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// floor(p / d) for p < 2^31, d < 2^17, given m = ceil(2^48 / d).
+__device__ __forceinline__ int div_m(int p, unsigned long long m)
+{
+    return (int)__umul64hi((unsigned long long)p, m << 16);
+}
+
 template <int CK, int BN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(320, 1)
 k_conv_gemm(const __grid_constant__ CUtensorMap tx, const __grid_constant__ CUtensorMap tw, GemmArgs a)
 {
     using Cfg = GemmCfg<CK, BN>;
-    constexpr int S = Cfg::STAGES;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *sm = smem_raw + (base - raw);
-    const uint32_t bar0 = base + S * Cfg::STAGE;   // full[S], empty[S], done
-    uint32_t *tslot = (uint32_t *)(sm + S * Cfg::STAGE + (2 * S + 1) * 8);
+    const int S = a.stages;
+    const uint32_t bres_off = (uint32_t)(S * a.stage_bytes);
+    const uint32_t bar_off = bres_off + (a.bres ? (uint32_t)(a.nkb * Cfg::B_AL) : 0u);
+    const uint32_t bar0 = base + bar_off;
     auto full = [&](int s) { return bar0 + 8u * s; };
     auto empty = [&](int s) { return bar0 + 8u * (S + s); };
-    const uint32_t done = bar0 + 8u * (2 * S);
-    auto sA = [&](int s) { return base + (uint32_t)(s * Cfg::STAGE); };
-    auto sB = [&](int s) { return base + (uint32_t)(s * Cfg::STAGE + Cfg::A_BYTES); };
+    const uint32_t bfull = bar0 + 16u * S;
+    auto tfull = [&](int b) { return bar0 + 16u * S + 8u + 8u * b; };
+    auto tempty = [&](int b) { return bar0 + 16u * S + 24u + 8u * b; };
+    uint32_t *tslot = (uint32_t *)(sm + bar_off + 16u * S + 40u);
+    float *sbias = (float *)(sm + bar_off + 16u * S + 64u);   // [Cout]
+    auto sA = [&](int s) { return base + (uint32_t)(s * a.stage_bytes); };
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p0 = blockIdx.x * 128;
-    const int co0 = blockIdx.y * BN;
+    for (int c = threadIdx.x; c < a.Cout; c += blockDim.x)
+        sbias[c] = a.bias ? a.bias[c] : 0.0f;
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) {
             mbar_init(full(s), 1);
             mbar_init(empty(s), 1);
         }
-        mbar_init(done, 1);
+        mbar_init(bfull, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(tfull(b), 1);
+            mbar_init(tempty(b), 128);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (warp == 0)
-        tmem_alloc(smem_u32(tslot), Cfg::TCOLS);
+        tmem_alloc(smem_u32(tslot), 2 * Cfg::TCOLS);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const int cpt = a.Cin / CK;
-    const int nk = 9 * cpt;
+    const int nkb = a.nkb;
 
-    if (warp == 0 && lane == 0) {
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % S;
-            if (kb >= S && !mbar_wait(empty(s), (uint32_t)((kb / S) - 1) & 1u)) {
-                set_err(1);
-                break;
+    // K order: groups of G taps x one channel block; group q covers taps
+    // G*(q / cpt) .. +G-1 of channel block q % cpt
+    const int ngrp = nkb / Cfg::G;
+    const bool one_ntile = a.ntiles == a.mtiles;
+    if (warp == 0) {
+        if (lane == 0) {
+            if (a.bres) {
+                mbar_expect_tx(bfull, (uint32_t)(nkb * Cfg::B_BYTES));
+                for (int kb = 0; kb < nkb; kb++) {
+                    const int tap = kb / cpt, c0 = (kb - tap * cpt) * CK;
+                    tma_load_2d(base + bres_off + (uint32_t)(kb * Cfg::B_AL), &tw, bfull,
+                                tap * a.Cin + c0, 0);
+                }
             }
-            const int tap = kb / cpt, c0 = (kb - tap * cpt) * CK;
-            const int shift = (tap / 3 - 1) * a.Wp + (tap % 3 - 1);
-            mbar_expect_tx(full(s), (uint32_t)Cfg::TX_BYTES);
-            tma_load_2d(sA(s), &tx, full(s), c0, p0 + shift);
-            tma_load_2d(sB(s), &tw, full(s), tap * a.Cin + c0, co0);
+            const uint32_t tx_bytes =
+                (uint32_t)(Cfg::G * (Cfg::A_BYTES + (a.bres ? 0 : Cfg::B_BYTES)));
+            int s = 0;
+            uint32_t ph = 0;            // ring round parity
+            bool wrapped = false;       // past the first round of the ring
+            bool bad = false;
+            for (int tile = blockIdx.x; tile < a.ntiles && !bad; tile += gridDim.x) {
+                int p0, co0;
+                if (one_ntile) {
+                    p0 = tile * 128;
+                    co0 = 0;
+                } else {
+                    const int nt = tile / a.mtiles;
+                    p0 = (tile - nt * a.mtiles) * 128;
+                    co0 = nt * BN;
+                }
+                int c0 = 0, tap0 = 0;
+                for (int qg = 0; qg < ngrp; qg++) {
+                    if (wrapped && !mbar_wait(empty(s), ph ^ 1u)) {
+                        set_err(1);
+                        bad = true;
+                        break;
+                    }
+                    mbar_expect_tx(full(s), tx_bytes);
+                    const uint32_t st = sA(s);
+#pragma unroll
+                    for (int g = 0; g < Cfg::G; g++) {
+                        const int tap = tap0 + g;
+                        const int ky = tap >= 6 ? 2 : tap >= 3 ? 1 : 0;
+                        const int shift = (ky - 1) * a.Wp + (tap - 3 * ky - 1);
+                        tma_load_2d(st + (uint32_t)(g * Cfg::A_BYTES), &tx, full(s), c0, p0 + shift);
+                        if (!a.bres)
+                            tma_load_2d(st + (uint32_t)(Cfg::G * Cfg::A_BYTES + g * Cfg::B_AL), &tw,
+                                        full(s), tap * a.Cin + c0, co0);
+                    }
+                    c0 += CK;
+                    if (c0 == a.Cin) {
+                        c0 = 0;
+                        tap0 += Cfg::G;
+                    }
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                        wrapped = true;
+                    }
+                }
+            }
         }
-    } else if (warp == 1 && lane == 0) {
-        constexpr uint32_t idesc = idesc_bf16(128, BN, false, false);
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % S;
-            if (!mbar_wait(full(s), (uint32_t)(kb / S) & 1u)) {
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(128, BN, false, false);
+            bool bad = a.bres && !mbar_wait(bfull, 0);
+            if (bad)
                 set_err(2);
+            int s = 0, tl = 0;
+            uint32_t ph = 0;
+            for (int tile = blockIdx.x; tile < a.ntiles && !bad; tile += gridDim.x, tl++) {
+                const int buf = tl & 1;
+                if (tl >= 2 && !mbar_wait(tempty(buf), (uint32_t)((tl >> 1) - 1) & 1u)) {
+                    set_err(2);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(buf * Cfg::TCOLS);
+                int cb = 0, tap0 = 0;
+                for (int qg = 0; qg < ngrp; qg++) {
+                    if (!mbar_wait(full(s), ph)) {
+                        set_err(2);
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = sA(s);
+#pragma unroll
+                    for (int g = 0; g < Cfg::G; g++) {
+                        const uint32_t ab = st + (uint32_t)(g * Cfg::A_BYTES);
+                        const uint32_t bb =
+                            a.bres ? base + bres_off + (uint32_t)(((tap0 + g) * cpt + cb) * Cfg::B_AL)
+                                   : st + (uint32_t)(Cfg::G * Cfg::A_BYTES + g * Cfg::B_AL);
+#pragma unroll
+                        for (int kk = 0; kk < CK / 16; kk++)
+                            umma_bf16(d, kdesc<CK>(ab + 32u * kk), kdesc<CK>(bb + 32u * kk), idesc,
+                                      (qg | g | kk) != 0 ? 1u : 0u);
+                    }
+                    umma_commit(empty(s));
+                    if (++cb == cpt) {
+                        cb = 0;
+                        tap0 += Cfg::G;
+                    }
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                umma_commit(tfull(buf));
+            }
+        }
+    } else {
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int grp = (warp - 2) >> 2;        // epilogue warpgroup = TMEM buffer
+        const int row = q * 32 + lane;
+        const int HW = a.Hp * a.Wp;
+        int k = 0;
+        for (int tile = blockIdx.x + grp * gridDim.x; tile < a.ntiles;
+             tile += 2 * gridDim.x, k++) {
+            if (!mbar_wait(tfull(grp), (uint32_t)k & 1u)) {
+                set_err(3);
                 break;
             }
+            __syncwarp();
             tc_fence_after();
-#pragma unroll
-            for (int kk = 0; kk < CK / 16; kk++) {
-                const uint64_t ad = smem_desc(sA(s) + 32u * kk, 16u, KSw<CK>::sbo, KSw<CK>::layout);
-                const uint64_t bd = smem_desc(sB(s) + 32u * kk, 16u, KSw<CK>::sbo, KSw<CK>::layout);
-                umma_bf16(tmem, ad, bd, idesc, (kb | kk) != 0 ? 1u : 0u);
+            const int p = (tile % a.mtiles) * 128 + row;
+            const int co0 = (tile / a.mtiles) * BN;
+            bool store = p < a.P;
+            if (store) {
+                const int qq = p - HW * div_m(p, a.m_hw);
+                const int yy = div_m(qq, a.m_w);
+                const int xx = qq - yy * a.Wp;
+                store = yy >= 1 && yy <= a.Hp - 2 && xx >= 1 && xx <= a.Wp - 2;
             }
-            umma_commit(empty(s));
-        }
-        umma_commit(done);
-    }
-    __syncwarp();
-    if (!mbar_wait(done, 0))
-        set_err(3);
-    __syncwarp();
-    tc_fence_after();
-
-    const int row = warp * 32 + lane;
-    const int p = p0 + row;
-    const bool store = interior(p, a.P, a.Hp, a.Wp);
+            const uint32_t t0 = tmem + (uint32_t)(grp * Cfg::TCOLS) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
-    for (int c = 0; c < BN; c += 32) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-        if (store && co0 + c < a.Cout) {
-            __align__(16) bf16 o[32];
+            for (int c = 0; c < BN; c += 32) {
+                float v[32];
+                tmem_ld32(t0 + (uint32_t)c, v);
+                if (store) {
+                    __align__(16) bf16 o[32];
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-                float x = v[j];
-                if (a.bias)
-                    x += a.bias[co0 + c + j];
-                if (a.relu)
-                    x = fmaxf(x, 0.0f);
-                o[j] = __float2bfloat16_rn(x);
+                    for (int j = 0; j < 32; j++) {
+                        float x = v[j] + sbias[co0 + c + j];
+                        if (a.relu)
+                            x = fmaxf(x, 0.0f);
+                        o[j] = __float2bfloat16_rn(x);
+                    }
+                    uint4 *dst = (uint4 *)(a.y + (size_t)p * a.Cout + co0 + c);
+                    const uint4 *src = (const uint4 *)o;
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        dst[j] = src[j];
+                }
             }
-            uint4 *dst = (uint4 *)(a.y + (size_t)p * a.Cout + co0 + c);
-            const uint4 *src = (const uint4 *)o;
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                dst[j] = src[j];
+            tc_fence_before();
+            mbar_arrive(tempty(grp));
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        tmem_dealloc(tmem, Cfg::TCOLS);
+        tmem_dealloc(tmem, 2 * Cfg::TCOLS);
 }
 
 // ---------------------------------------------------------------------------
@@ -448,133 +584,205 @@ __device__ __forceinline__ long long prow(int n, int y, int x, int H, int W)
     return ((long long)n * (H + 2) + y + 1) * (W + 2) + x + 1;
 }
 
-// 2x2 max pooling; idx keeps the arg max (0..3) for the backward pass.
-__global__ void k_maxpool2(const bf16 *x, bf16 *y, uint8_t *idx, int N, int H, int W, int C)
+// Pixel-wise layers move 16-byte vectors of 8 bf16 channels (C is a
+// multiple of 16); index arithmetic is per vector, in 32 bits.
+__device__ __forceinline__ void unpack8(uint4 u, float (&f)[8])
+{
+    const __nv_bfloat162 *h = (const __nv_bfloat162 *)&u;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float2 t = __bfloat1622float2(h[k]);
+        f[2 * k] = t.x;
+        f[2 * k + 1] = t.y;
+    }
+}
+
+__device__ __forceinline__ uint4 pack8(const float (&f)[8])
+{
+    uint4 u;
+    __nv_bfloat162 *h = (__nv_bfloat162 *)&u;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+    return u;
+}
+
+#define FCAB_GRID_LOOP(i, total)                                                      \
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (total); i += gridDim.x * blockDim.x)
+
+// 2x2 max pooling of an (H, W) image (V vectors per pixel); idx keeps the
+// arg max (0..3, first maximum) of every channel for the backward pass.
+__global__ void k_maxpool2(const uint4 *x, uint4 *y, uint2 *idx, int N, int H, int W, int V)
 {
     const int Ho = H / 2, Wo = W / 2;
-    const long long total = (long long)N * Ho * Wo * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        long long t = i / C;
-        const int ox = (int)(t % Wo);
+    FCAB_GRID_LOOP(i, N * Ho * Wo * V)
+    {
+        const int v = i % V;
+        int t = i / V;
+        const int ox = t % Wo;
         t /= Wo;
-        const int oy = (int)(t % Ho);
-        const int n = (int)(t / Ho);
-        float best = -INFINITY;
-        int bi = 0;
+        const int oy = t % Ho;
+        const int n = t / Ho;
+        float best[8], cur[8];
+        uint32_t arg[8];
+        unpack8(x[prow(n, 2 * oy, 2 * ox, H, W) * V + v], best);
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            arg[c] = 0;
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            unpack8(x[prow(n, 2 * oy + (k >> 1), 2 * ox + (k & 1), H, W) * V + v], cur);
+#pragma unroll
+            for (int c = 0; c < 8; c++)
+                if (cur[c] > best[c]) {
+                    best[c] = cur[c];
+                    arg[c] = k;
+                }
+        }
+        y[prow(n, oy, ox, Ho, Wo) * V + v] = pack8(best);
+        uint2 a;
+        a.x = arg[0] | arg[1] << 8 | arg[2] << 16 | arg[3] << 24;
+        a.y = arg[4] | arg[5] << 8 | arg[6] << 16 | arg[7] << 24;
+        idx[i] = a;
+    }
+}
+
+// Gradient of the pooling: each input pixel gets dy where it was the arg
+// max, else 0; plus, when add is given, add[p][aoff + ...] (row width aV
+// vectors): the skip connection's gradient taken straight from the
+// concatenation's gradient.
+__global__ void k_maxpool2_bwd(const uint4 *dy, const uint2 *idx, const uint4 *add, int aV, int aoff,
+                               uint4 *dx, int N, int H, int W, int V)
+{
+    const int Ho = H / 2, Wo = W / 2;
+    FCAB_GRID_LOOP(i, N * Ho * Wo * V)
+    {
+        const int v = i % V;
+        int t = i / V;
+        const int ox = t % Wo;
+        t /= Wo;
+        const int oy = t % Ho;
+        const int n = t / Ho;
+        float g[8];
+        unpack8(dy[prow(n, oy, ox, Ho, Wo) * V + v], g);
+        const uint2 a = idx[i];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            const float v = __bfloat162float(x[prow(n, 2 * oy + (k >> 1), 2 * ox + (k & 1), H, W) * C + c]);
-            if (v > best) {
-                best = v;
-                bi = k;
+            const long long p = prow(n, 2 * oy + (k >> 1), 2 * ox + (k & 1), H, W);
+            float o[8], ad[8];
+            if (add)
+                unpack8(add[p * aV + aoff + v], ad);
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const uint32_t ac = ((c < 4 ? a.x : a.y) >> (8 * (c & 3))) & 0xffu;
+                o[c] = ac == (uint32_t)k ? g[c] : 0.0f;
+                if (add)
+                    o[c] += ad[c];
             }
+            dx[p * V + v] = pack8(o);
         }
-        y[prow(n, oy, ox, Ho, Wo) * C + c] = __float2bfloat16_rn(best);
-        idx[i] = (uint8_t)bi;
     }
 }
 
-__global__ void k_maxpool2_bwd(const bf16 *dy, const uint8_t *idx, bf16 *dx, int N, int H, int W, int C)
+// y = [a | b] over the interior pixels of an (H, W) image; a is read at
+// half resolution (nearest 2x upsampling) when a_half != 0. Vb = 0 gives
+// the plain upsampling.
+__global__ void k_cat2(const uint4 *a, int Va, int a_half, const uint4 *b, int Vb, uint4 *y, int N,
+                       int H, int W)
 {
-    const int Ho = H / 2, Wo = W / 2;
-    const long long total = (long long)N * Ho * Wo * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        long long t = i / C;
-        const int ox = (int)(t % Wo);
-        t /= Wo;
-        const int oy = (int)(t % Ho);
-        const int n = (int)(t / Ho);
-        const bf16 g = dy[prow(n, oy, ox, Ho, Wo) * C + c];
-        const int bi = idx[i];
-        const bf16 z = __float2bfloat16_rn(0.0f);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            dx[prow(n, 2 * oy + (k >> 1), 2 * ox + (k & 1), H, W) * C + c] = k == bi ? g : z;
-    }
-}
-
-// Nearest-neighbour 2x upsampling of an (H, W) image to (2H, 2W).
-__global__ void k_upsample2(const bf16 *x, bf16 *y, int N, int H, int W, int C)
-{
-    const int Ho = 2 * H, Wo = 2 * W;
-    const long long total = (long long)N * Ho * Wo * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        long long t = i / C;
-        const int ox = (int)(t % Wo);
-        t /= Wo;
-        const int oy = (int)(t % Ho);
-        const int n = (int)(t / Ho);
-        y[prow(n, oy, ox, Ho, Wo) * C + c] = x[prow(n, oy >> 1, ox >> 1, H, W) * C + c];
-    }
-}
-
-// Gradient of the upsampling: each (H, W) pixel sums its four children.
-__global__ void k_upsample2_bwd(const bf16 *dy, bf16 *dx, int N, int H, int W, int C)
-{
-    const long long total = (long long)N * H * W * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        long long t = i / C;
-        const int x = (int)(t % W);
+    const int V = Va + Vb;
+    FCAB_GRID_LOOP(i, N * H * W * V)
+    {
+        const int v = i % V;
+        int t = i / V;
+        const int x = t % W;
         t /= W;
-        const int y = (int)(t % H);
-        const int n = (int)(t / H);
-        float s = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-            s += __bfloat162float(dy[prow(n, 2 * y + (k >> 1), 2 * x + (k & 1), 2 * H, 2 * W) * C + c]);
-        dx[prow(n, y, x, H, W) * C + c] = __float2bfloat16_rn(s);
-    }
-}
-
-// Channel concatenation [a | b] over the interior pixels (and its split).
-__global__ void k_concat(const bf16 *a, int Ca, const bf16 *b, int Cb, bf16 *y, int N, int H, int W,
-                         int backward)
-{
-    const int C = Ca + Cb;
-    const long long total = (long long)N * H * W * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        long long t = i / C;
-        const int x = (int)(t % W);
-        t /= W;
-        const int yy = (int)(t % H);
-        const int n = (int)(t / H);
+        const int yy = t % H;
+        const int n = t / H;
         const long long r = prow(n, yy, x, H, W);
-        if (!backward) {
-            y[r * C + c] = c < Ca ? a[r * Ca + c] : b[r * Cb + (c - Ca)];
-        } else {
-            if (c < Ca)
-                ((bf16 *)a)[r * Ca + c] = y[r * C + c];
-            else
-                ((bf16 *)b)[r * Cb + (c - Ca)] = y[r * C + c];
-        }
+        uint4 val;
+        if (v < Va)
+            val = a_half ? a[prow(n, yy >> 1, x >> 1, H >> 1, W >> 1) * Va + v] : a[r * Va + v];
+        else
+            val = b[r * Vb + (v - Va)];
+        y[r * V + v] = val;
     }
 }
 
-// y += x (bf16, FP32 sum).
-__global__ void k_add(bf16 *y, const bf16 *x, long long n)
+// Split of a concatenation's gradient y = [a | b] (same resolution).
+__global__ void k_split(const uint4 *y, uint4 *a, int Va, uint4 *b, int Vb, int N, int H, int W)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-        y[i] = __float2bfloat16_rn(__bfloat162float(y[i]) + __bfloat162float(x[i]));
+    const int V = Va + Vb;
+    FCAB_GRID_LOOP(i, N * H * W * V)
+    {
+        const int v = i % V;
+        int t = i / V;
+        const int x = t % W;
+        t /= W;
+        const int yy = t % H;
+        const int n = t / H;
+        const long long r = prow(n, yy, x, H, W);
+        if (v < Va)
+            a[r * Va + v] = y[r * V + v];
+        else
+            b[r * Vb + (v - Va)] = y[r * V + v];
+    }
 }
 
-// g *= (y > 0) over the whole matrix (borders are zero in g).
-__global__ void k_relu_bwd(bf16 *g, const bf16 *y, long long n)
+// Gradient of the nearest 2x upsampling: dx (H, W, V vectors) sums the four
+// children in dy (2H, 2W; row width sV vectors, first V of them used).
+__global__ void k_upsum(const uint4 *dy, int sV, uint4 *dx, int N, int H, int W, int V)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+    FCAB_GRID_LOOP(i, N * H * W * V)
+    {
+        const int v = i % V;
+        int t = i / V;
+        const int x = t % W;
+        t /= W;
+        const int yy = t % H;
+        const int n = t / H;
+        float s[8], c[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            s[j] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            unpack8(dy[prow(n, 2 * yy + (k >> 1), 2 * x + (k & 1), 2 * H, 2 * W) * sV + v], c);
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                s[j] += c[j];
+        }
+        dx[prow(n, yy, x, H, W) * V + v] = pack8(s);
+    }
+}
+
+// y += x (FP32 sum), n8 vectors.
+__global__ void k_add(uint4 *y, const uint4 *x, long long n8)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n8;
          i += (long long)gridDim.x * blockDim.x) {
-        if (!(__bfloat162float(y[i]) > 0.0f))
-            g[i] = __float2bfloat16_rn(0.0f);
+        float a[8], b[8];
+        unpack8(y[i], a);
+        unpack8(x[i], b);
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            a[j] += b[j];
+        y[i] = pack8(a);
+    }
+}
+
+// g *= (y > 0) over the whole matrix (borders are zero in g), n8 vectors.
+__global__ void k_relu_bwd(uint4 *g, const uint4 *y, long long n8)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n8;
+         i += (long long)gridDim.x * blockDim.x) {
+        float a[8], b[8];
+        unpack8(g[i], a);
+        unpack8(y[i], b);
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            a[j] = b[j] > 0.0f ? a[j] : 0.0f;
+        g[i] = pack8(a);
     }
 }
 
@@ -588,18 +796,25 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x)
     return x;
 }
 
-// Inverted dropout in place: keep with probability 1-p, scale kept by
-// 1/(1-p). The mask is a hash of (seed, element), so the backward pass
-// regenerates it. Border pixels stay zero.
-__global__ void k_dropout(bf16 *x, long long n, float p, uint32_t seed)
+// Inverted dropout in place: element e is kept when hash(seed, e) >= p*2^32,
+// kept values scaled by 1/(1-p). The backward pass regenerates the mask with
+// the same seed. Border pixels stay zero.
+__global__ void k_dropout(uint4 *x, long long n8, float p, uint32_t seed)
 {
     const uint32_t thr = (uint32_t)(p * 4294967296.0);
     const float scale = 1.0f / (1.0f - p);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+    const uint32_t hs = hash32(seed);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n8;
          i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t h = hash32((uint32_t)i ^ hash32(seed + (uint32_t)(i >> 32) * 0x9e3779b9U));
-        const float v = __bfloat162float(x[i]);
-        x[i] = __float2bfloat16_rn(h >= thr ? v * scale : 0.0f);
+        float a[8];
+        unpack8(x[i], a);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const long long e = i * 8 + j;
+            const uint32_t h = hash32((uint32_t)e ^ hash32(hs + (uint32_t)(e >> 32) * 0x9e3779b9U));
+            a[j] = h >= thr ? a[j] * scale : 0.0f;
+        }
+        x[i] = pack8(a);
     }
 }
 
@@ -618,63 +833,86 @@ __global__ void k_bias_grad(const bf16 *g, long long P, int C, float *db)
 }
 
 // Output head: 1x1 convolution C -> 1, FP32 result on the unpadded grid.
-__global__ void k_head_fwd(const bf16 *x, const float *w, const float *b, float *out, int N, int H,
-                           int W, int C)
+template <int C>
+__global__ void k_head_fwd(const uint4 *x, const float *w, const float *b, float *out, int N, int H,
+                           int W)
 {
-    const long long total = (long long)N * H * W;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int xx = (int)(i % W);
-        const long long t = i / W;
-        const int yy = (int)(t % H);
-        const int n = (int)(t / H);
-        const bf16 *r = x + prow(n, yy, xx, H, W) * C;
+    constexpr int V = C / 8;
+    FCAB_GRID_LOOP(i, N * H * W)
+    {
+        const int xx = i % W;
+        const int t = i / W;
+        const int yy = t % H;
+        const int n = t / H;
+        const long long r = prow(n, yy, xx, H, W) * V;
         float s = b[0];
-        for (int c = 0; c < C; c++)
-            s += w[c] * __bfloat162float(r[c]);
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            float f[8];
+            unpack8(x[r + v], f);
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                s += w[v * 8 + j] * f[j];
+        }
         out[i] = s;
     }
 }
 
 // Mean squared error of the head against the target, and its gradients:
-// dx (bf16, padded), dw[c], db (accumulated), loss (accumulated sum).
-__global__ void k_head_bwd(const bf16 *x, const float *w, const float *out, const float *target,
-                           bf16 *dx, float *dw, float *db, float *loss, int N, int H, int W, int C,
+// dx (bf16, bordered), dw[c], db, loss sum (accumulated). Each thread keeps
+// its dw partial sums in registers; warps reduce them before the atomics.
+template <int C>
+__global__ void k_head_bwd(const uint4 *x, const float *w, const float *out, const float *target,
+                           uint4 *dx, float *dw, float *db, float *loss, int N, int H, int W,
                            float inv_count)
 {
-    __shared__ float s_dw[256];
-    __shared__ float s_db, s_loss;
-    for (int c = threadIdx.x; c < C; c += blockDim.x)
-        s_dw[c] = 0.0f;
-    if (threadIdx.x == 0)
-        s_db = s_loss = 0.0f;
-    __syncthreads();
-    const long long total = (long long)N * H * W;
+    constexpr int V = C / 8;
+    float acc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++)
+        acc[c] = 0.0f;
     float ldb = 0.0f, lloss = 0.0f;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int xx = (int)(i % W);
-        const long long t = i / W;
-        const int yy = (int)(t % H);
-        const int n = (int)(t / H);
-        const long long r = prow(n, yy, xx, H, W) * C;
+    FCAB_GRID_LOOP(i, N * H * W)
+    {
+        const int xx = i % W;
+        const int t = i / W;
+        const int yy = t % H;
+        const int n = t / H;
+        const long long r = prow(n, yy, xx, H, W) * V;
         const float e = out[i] - target[i];
         lloss += e * e;
         const float d = 2.0f * e * inv_count;
         ldb += d;
-        for (int c = 0; c < C; c++) {
-            dx[r + c] = __float2bfloat16_rn(d * w[c]);
-            atomicAdd(&s_dw[c], d * __bfloat162float(x[r + c]));
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            float f[8], o[8];
+            unpack8(x[r + v], f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                acc[v * 8 + j] += d * f[j];
+                o[j] = d * w[v * 8 + j];
+            }
+            dx[r + v] = pack8(o);
         }
     }
-    atomicAdd(&s_db, ldb);
-    atomicAdd(&s_loss, lloss);
-    __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x)
-        atomicAdd(dw + c, s_dw[c]);
-    if (threadIdx.x == 0) {
-        atomicAdd(db, s_db);
-        atomicAdd(loss, s_loss);
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        float s = acc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0)
+            atomicAdd(dw + c, s);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ldb += __shfl_xor_sync(0xffffffffu, ldb, o);
+        lloss += __shfl_xor_sync(0xffffffffu, lloss, o);
+    }
+    if (lane == 0) {
+        atomicAdd(db, ldb);
+        atomicAdd(loss, lloss);
     }
 }
 
@@ -710,20 +948,25 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, long long n
     }
 }
 
-// FP32 inputs [N][H][W][Cs] -> bf16 padded matrix with C >= Cs channels.
-__global__ void k_pack_input(const float *in, int Cs, bf16 *x, int C, int N, int H, int W)
+// FP32 inputs [N][H][W][Cs] -> bf16 bordered matrix with C >= Cs channels.
+__global__ void k_pack_input(const float *in, int Cs, uint4 *x, int C, int N, int H, int W)
 {
-    const long long total = (long long)N * H * W * C;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const long long t = i / C;
-        const int xx = (int)(t % W);
-        const long long t2 = t / W;
-        const int yy = (int)(t2 % H);
-        const int n = (int)(t2 / H);
-        const float v = c < Cs ? in[t * Cs + c] : 0.0f;
-        x[prow(n, yy, xx, H, W) * C + c] = __float2bfloat16_rn(v);
+    const int V = C / 8;
+    FCAB_GRID_LOOP(i, N * H * W * V)
+    {
+        const int v = i % V;
+        const int t = i / V;
+        const int xx = t % W;
+        const int t2 = t / W;
+        const int yy = t2 % H;
+        const int n = t2 / H;
+        float f[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = v * 8 + j;
+            f[j] = c < Cs ? in[(long long)t * Cs + c] : 0.0f;
+        }
+        x[prow(n, yy, xx, H, W) * V + v] = pack8(f);
     }
 }
 
@@ -767,37 +1010,54 @@ bool make_map(CUtensorMap *m, const void *ptr, long long rows, int cols, int bc,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+constexpr int SMEM_MAX = 232448;   // per-CTA dynamic shared memory limit (227 KB)
+
 template <int CK, int BN>
-cudaError_t launch_gemm(const CUtensorMap &tx, const CUtensorMap &tw, const GemmArgs &a, int n_tiles,
-                        cudaStream_t st)
+cudaError_t launch_gemm(const CUtensorMap &tx, const CUtensorMap &tw, GemmArgs a, cudaStream_t st)
 {
     using Cfg = GemmCfg<CK, BN>;
-    static bool attr_set[64] = {};
+    // resident weights when they take at most 96 KB and there is one
+    // channel tile; the A ring gets what is left (at most 8 stages)
+    const int bres_bytes = a.nkb * Cfg::B_AL;
+    a.bres = (a.ntiles == a.mtiles && bres_bytes <= 98304) ? 1 : 0;
+    a.stage_bytes = Cfg::G * (Cfg::A_BYTES + (a.bres ? 0 : Cfg::B_AL));
+    // as many stages as fit (the loads in flight hide the L2 latency of the
+    // nine shifted tap tiles); barrier area 16 B per stage + 64 B
+    const int fixed = 1024 + (a.bres ? bres_bytes : 0) + 64 + 4 * a.Cout;
+    int stages = (SMEM_MAX - fixed) / (a.stage_bytes + 16);
+    stages = stages > 32 ? 32 : stages;
+    if (stages < 2)
+        return cudaErrorInvalidValue;
+    a.stages = stages;
+    const int smem = fixed + stages * (a.stage_bytes + 16);
+    static int attr_smem[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!attr_set[dev & 63]) {
+    if (attr_smem[dev & 63] < smem) {
         cudaError_t e = cudaFuncSetAttribute(k_conv_gemm<CK, BN>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_MAX);
         if (e != cudaSuccess)
             return e;
-        attr_set[dev & 63] = true;
+        attr_smem[dev & 63] = SMEM_MAX;
     }
-    dim3 grid((unsigned)((a.P + 127) / 128), (unsigned)n_tiles);
-    k_conv_gemm<CK, BN><<<grid, 128, Cfg::SMEM, st>>>(tx, tw, a);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = a.ntiles < nsm ? a.ntiles : nsm;
+    k_conv_gemm<CK, BN><<<grid, 320, smem, st>>>(tx, tw, a);
     return cudaGetLastError();
 }
 
 template <int CK>
 cudaError_t gemm_bn(const CUtensorMap &tx, const CUtensorMap &tw, const GemmArgs &a, int bn,
-                    int n_tiles, cudaStream_t st)
+                    cudaStream_t st)
 {
     switch (bn) {
-    case 32: return launch_gemm<CK, 32>(tx, tw, a, n_tiles, st);
-    case 64: return launch_gemm<CK, 64>(tx, tw, a, n_tiles, st);
-    case 96: return launch_gemm<CK, 96>(tx, tw, a, n_tiles, st);
-    case 128: return launch_gemm<CK, 128>(tx, tw, a, n_tiles, st);
-    case 192: return launch_gemm<CK, 192>(tx, tw, a, n_tiles, st);
-    case 256: return launch_gemm<CK, 256>(tx, tw, a, n_tiles, st);
+    case 32: return launch_gemm<CK, 32>(tx, tw, a, st);
+    case 64: return launch_gemm<CK, 64>(tx, tw, a, st);
+    case 96: return launch_gemm<CK, 96>(tx, tw, a, st);
+    case 128: return launch_gemm<CK, 128>(tx, tw, a, st);
+    case 192: return launch_gemm<CK, 192>(tx, tw, a, st);
+    case 256: return launch_gemm<CK, 256>(tx, tw, a, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -815,8 +1075,8 @@ int conv_gemm(const void *x, int N, int H, int W, int Cin, const void *w, int Co
     if (Cout % bn || bn % 32)
         return fail(FCAB_ERR_ARG, "conv: unsupported Cout");
     const long long P = (long long)N * (H + 2) * (W + 2);
-    if (P >= (1ll << 31) - 256)
-        return fail(FCAB_ERR_ARG, "conv: too many pixels");
+    if (P >= (1ll << 31) - 256 || (long long)(H + 2) * (W + 2) >= (1 << 17) || Cout > 384)
+        return fail(FCAB_ERR_ARG, "conv: too many pixels or channels");
     const CUtensorMapSwizzle sw = CK == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
                                   : CK == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
                                              : CU_TENSOR_MAP_SWIZZLE_32B;
@@ -829,12 +1089,20 @@ int conv_gemm(const void *x, int N, int H, int W, int Cin, const void *w, int Co
     a.Wp = W + 2;
     a.Cin = Cin;
     a.Cout = Cout;
+    a.mtiles = (int)((P + 127) / 128);
+    a.ntiles = a.mtiles * (Cout / bn);
+    a.nkb = 9 * (Cin / CK);
+    a.bres = 0;
+    a.stages = 0;
+    a.stage_bytes = 0;
+    a.m_hw = ((1ull << 48) + (unsigned long long)(a.Hp * a.Wp) - 1) / (unsigned long long)(a.Hp * a.Wp);
+    a.m_w = ((1ull << 48) + (unsigned long long)a.Wp - 1) / (unsigned long long)a.Wp;
     a.bias = bias;
     a.y = (bf16 *)y;
     a.relu = relu;
-    cudaError_t e = CK == 64 ? gemm_bn<64>(tx, tw, a, bn, Cout / bn, st)
-                    : CK == 32 ? gemm_bn<32>(tx, tw, a, bn, Cout / bn, st)
-                               : gemm_bn<16>(tx, tw, a, bn, Cout / bn, st);
+    cudaError_t e = CK == 64 ? gemm_bn<64>(tx, tw, a, bn, st)
+                    : CK == 32 ? gemm_bn<32>(tx, tw, a, bn, st)
+                               : gemm_bn<16>(tx, tw, a, bn, st);
     if (e != cudaSuccess)
         return fail(FCAB_ERR_CUDA, cudaGetErrorString(e));
     return 0;
@@ -935,53 +1203,113 @@ int fcab_unet_conv_wgrad(const void *dy, const void *x, int N, int H, int W, int
         return 0;                                                                      \
     } while (0)
 
+static bool fits32(long long n) { return n >= 0 && n < (1ll << 31); }
+
+#define FCAB_CHECK_VEC(C, n)                                                          \
+    do {                                                                              \
+        if ((C) % 8 || !fits32(n))                                                    \
+            return fail(FCAB_ERR_ARG, "channels must be a multiple of 8 and sizes < 2^31"); \
+    } while (0)
+
 int fcab_unet_maxpool2(const void *x, void *y, uint8_t *idx, int N, int H, int W, int C, void *stream)
 {
     if (H % 2 || W % 2)
         return fail(FCAB_ERR_ARG, "maxpool2: H and W must be even");
-    FCAB_EW_LAUNCH(k_maxpool2, (long long)N * (H / 2) * (W / 2) * C, (const bf16 *)x, (bf16 *)y, idx,
-                   N, H, W, C);
+    const long long n = (long long)N * (H / 2) * (W / 2) * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    FCAB_EW_LAUNCH(k_maxpool2, n, (const uint4 *)x, (uint4 *)y, (uint2 *)idx, N, H, W, C / 8);
 }
 
 int fcab_unet_maxpool2_bwd(const void *dy, const uint8_t *idx, void *dx, int N, int H, int W, int C,
                            void *stream)
 {
-    FCAB_EW_LAUNCH(k_maxpool2_bwd, (long long)N * (H / 2) * (W / 2) * C, (const bf16 *)dy, idx,
-                   (bf16 *)dx, N, H, W, C);
+    const long long n = (long long)N * (H / 2) * (W / 2) * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    FCAB_EW_LAUNCH(k_maxpool2_bwd, n, (const uint4 *)dy, (const uint2 *)idx, (const uint4 *)nullptr,
+                   0, 0, (uint4 *)dx, N, H, W, C / 8);
+}
+
+int fcab_unet_maxpool2_bwd_add(const void *dy, const uint8_t *idx, const void *add, int Cadd,
+                               int add_off, void *dx, int N, int H, int W, int C, void *stream)
+{
+    const long long n = (long long)N * (H / 2) * (W / 2) * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    if (Cadd % 8 || add_off % 8 || add_off + C > Cadd)
+        return fail(FCAB_ERR_ARG, "maxpool2_bwd_add: bad channel slice");
+    FCAB_EW_LAUNCH(k_maxpool2_bwd, n, (const uint4 *)dy, (const uint2 *)idx, (const uint4 *)add,
+                   Cadd / 8, add_off / 8, (uint4 *)dx, N, H, W, C / 8);
 }
 
 int fcab_unet_upsample2(const void *x, void *y, int N, int H, int W, int C, void *stream)
 {
-    FCAB_EW_LAUNCH(k_upsample2, (long long)N * 4 * H * W * C, (const bf16 *)x, (bf16 *)y, N, H, W, C);
+    const long long n = (long long)N * 4 * H * W * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    FCAB_EW_LAUNCH(k_cat2, n, (const uint4 *)x, C / 8, 1, (const uint4 *)nullptr, 0, (uint4 *)y, N,
+                   2 * H, 2 * W);
 }
 
 int fcab_unet_upsample2_bwd(const void *dy, void *dx, int N, int H, int W, int C, void *stream)
 {
-    FCAB_EW_LAUNCH(k_upsample2_bwd, (long long)N * H * W * C, (const bf16 *)dy, (bf16 *)dx, N, H, W, C);
+    const long long n = (long long)N * H * W * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    FCAB_EW_LAUNCH(k_upsum, n, (const uint4 *)dy, C / 8, (uint4 *)dx, N, H, W, C / 8);
 }
 
 int fcab_unet_concat(const void *a, int Ca, const void *b, int Cb, void *y, int N, int H, int W,
                      int backward, void *stream)
 {
-    FCAB_EW_LAUNCH(k_concat, (long long)N * H * W * (Ca + Cb), (const bf16 *)a, Ca, (const bf16 *)b,
-                   Cb, (bf16 *)y, N, H, W, backward);
+    const long long n = (long long)N * H * W * ((Ca + Cb) / 8);
+    FCAB_CHECK_VEC(Ca, n);
+    FCAB_CHECK_VEC(Cb, n);
+    if (!backward)
+        FCAB_EW_LAUNCH(k_cat2, n, (const uint4 *)a, Ca / 8, 0, (const uint4 *)b, Cb / 8, (uint4 *)y,
+                       N, H, W);
+    FCAB_EW_LAUNCH(k_split, n, (const uint4 *)y, (uint4 *)a, Ca / 8, (uint4 *)b, Cb / 8, N, H, W);
+}
+
+int fcab_unet_upcat(const void *coarse, int C1, const void *skip, int C2, void *y, int N, int H,
+                    int W, void *stream)
+{
+    if (H % 2 || W % 2)
+        return fail(FCAB_ERR_ARG, "upcat: H and W must be even");
+    const long long n = (long long)N * H * W * ((C1 + C2) / 8);
+    FCAB_CHECK_VEC(C1, n);
+    FCAB_CHECK_VEC(C2, n);
+    FCAB_EW_LAUNCH(k_cat2, n, (const uint4 *)coarse, C1 / 8, 1, (const uint4 *)skip, C2 / 8,
+                   (uint4 *)y, N, H, W);
+}
+
+int fcab_unet_upcat_bwd(const void *gy, int C1, int C2, void *gcoarse, int N, int H, int W,
+                        void *stream)
+{
+    if (H % 2 || W % 2)
+        return fail(FCAB_ERR_ARG, "upcat_bwd: H and W must be even");
+    const long long n = (long long)N * (H / 2) * (W / 2) * (C1 / 8);
+    FCAB_CHECK_VEC(C1, n);
+    FCAB_CHECK_VEC(C2, n);
+    FCAB_EW_LAUNCH(k_upsum, n, (const uint4 *)gy, (C1 + C2) / 8, (uint4 *)gcoarse, N, H / 2, W / 2,
+                   C1 / 8);
 }
 
 int fcab_unet_add(void *y, const void *x, long long n, void *stream)
 {
-    FCAB_EW_LAUNCH(k_add, n, (bf16 *)y, (const bf16 *)x, n);
+    if (n % 8)
+        return fail(FCAB_ERR_ARG, "add: n must be a multiple of 8");
+    FCAB_EW_LAUNCH(k_add, n / 8, (uint4 *)y, (const uint4 *)x, n / 8);
 }
 
 int fcab_unet_relu_bwd(void *g, const void *y, long long n, void *stream)
 {
-    FCAB_EW_LAUNCH(k_relu_bwd, n, (bf16 *)g, (const bf16 *)y, n);
+    if (n % 8)
+        return fail(FCAB_ERR_ARG, "relu_bwd: n must be a multiple of 8");
+    FCAB_EW_LAUNCH(k_relu_bwd, n / 8, (uint4 *)g, (const uint4 *)y, n / 8);
 }
 
 int fcab_unet_dropout(void *x, long long n, float p, uint32_t seed, void *stream)
 {
-    if (!(p >= 0.0f && p < 1.0f))
-        return fail(FCAB_ERR_ARG, "dropout: p must be in [0, 1)");
-    FCAB_EW_LAUNCH(k_dropout, n, (bf16 *)x, n, p, seed);
+    if (!(p >= 0.0f && p < 1.0f) || n % 8)
+        return fail(FCAB_ERR_ARG, "dropout: p must be in [0, 1) and n a multiple of 8");
+    FCAB_EW_LAUNCH(k_dropout, n / 8, (uint4 *)x, n / 8, p, seed);
 }
 
 int fcab_unet_bias_grad(const void *g, long long P, int C, float *db, void *stream)
@@ -1001,18 +1329,31 @@ int fcab_unet_bias_grad(const void *g, long long P, int C, float *db, void *stre
 int fcab_unet_head_fwd(const void *x, const float *w, const float *b, float *out, int N, int H,
                        int W, int C, void *stream)
 {
-    FCAB_EW_LAUNCH(k_head_fwd, (long long)N * H * W, (const bf16 *)x, w, b, out, N, H, W, C);
+    const long long n = (long long)N * H * W;
+    if (!fits32(n))
+        return fail(FCAB_ERR_ARG, "head: too many pixels");
+    if (C == 32)
+        FCAB_EW_LAUNCH(k_head_fwd<32>, n, (const uint4 *)x, w, b, out, N, H, W);
+    if (C == 64)
+        FCAB_EW_LAUNCH(k_head_fwd<64>, n, (const uint4 *)x, w, b, out, N, H, W);
+    return fail(FCAB_ERR_ARG, "head: C must be 32 or 64");
 }
 
 int fcab_unet_head_bwd(const void *x, const float *w, const float *out, const float *target,
                        void *dx, float *dw, float *db, float *loss, int N, int H, int W, int C,
                        void *stream)
 {
-    if (C > 256)
-        return fail(FCAB_ERR_ARG, "head: C must be <= 256");
-    const float inv = 1.0f / (float)((long long)N * H * W);
-    FCAB_EW_LAUNCH(k_head_bwd, (long long)N * H * W, (const bf16 *)x, w, out, target, (bf16 *)dx, dw,
-                   db, loss, N, H, W, C, inv);
+    const long long n = (long long)N * H * W;
+    if (!fits32(n))
+        return fail(FCAB_ERR_ARG, "head: too many pixels");
+    const float inv = 1.0f / (float)n;
+    if (C == 32)
+        FCAB_EW_LAUNCH(k_head_bwd<32>, n, (const uint4 *)x, w, out, target, (uint4 *)dx, dw, db,
+                       loss, N, H, W, inv);
+    if (C == 64)
+        FCAB_EW_LAUNCH(k_head_bwd<64>, n, (const uint4 *)x, w, out, target, (uint4 *)dx, dw, db,
+                       loss, N, H, W, inv);
+    return fail(FCAB_ERR_ARG, "head: C must be 32 or 64");
 }
 
 int fcab_unet_prep_weights(const float *w, void *wb, void *wt, int Cout, int Cin, void *stream)
@@ -1031,7 +1372,9 @@ int fcab_unet_pack_input(const float *in, int Cs, void *x, int C, int N, int H, 
 {
     if (Cs > C)
         return fail(FCAB_ERR_ARG, "pack_input: more source channels than matrix channels");
-    FCAB_EW_LAUNCH(k_pack_input, (long long)N * H * W * C, in, Cs, (bf16 *)x, C, N, H, W);
+    const long long n = (long long)N * H * W * (C / 8);
+    FCAB_CHECK_VEC(C, n);
+    FCAB_EW_LAUNCH(k_pack_input, n, in, Cs, (uint4 *)x, C, N, H, W);
 }
 
 // Returns and clears the device error code of the surrogate kernels (0: none).

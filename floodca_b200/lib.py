@@ -77,6 +77,9 @@ def core() -> C.CDLL:
         "fcab_unet_conv_wgrad": (C.c_int, [_P, _P, _I, _I, _I, _I, _I, _P, _P]),
         "fcab_unet_maxpool2": (C.c_int, [_P, _P, _P, _I, _I, _I, _I, _P]),
         "fcab_unet_maxpool2_bwd": (C.c_int, [_P, _P, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_maxpool2_bwd_add": (C.c_int, [_P, _P, _P, _I, _I, _P, _I, _I, _I, _I, _P]),
+        "fcab_unet_upcat": (C.c_int, [_P, _I, _P, _I, _P, _I, _I, _I, _P]),
+        "fcab_unet_upcat_bwd": (C.c_int, [_P, _I, _I, _P, _I, _I, _I, _P]),
         "fcab_unet_upsample2": (C.c_int, [_P, _P, _I, _I, _I, _I, _P]),
         "fcab_unet_upsample2_bwd": (C.c_int, [_P, _P, _I, _I, _I, _I, _P]),
         "fcab_unet_concat": (C.c_int, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P]),

@@ -192,10 +192,93 @@ def screen(model, X, passes: int = 8, area_thr_cells: int | None = None,
             "t_surrogate_s": t_sur, "spread": spread.cpu().numpy(), "area": area.cpu().numpy()}
 
 
+def layer_bench(N: int = 64, steps: int = 10, warmup: int = 3, train_batch: int = 32) -> dict:
+    """Device time of MC-dropout forward passes (N images) and of training
+    steps (forward, backward, Adam) on random inputs, CUDA events on the
+    current stream."""
+    import torch
+    from .unet import UNet
+    model = UNet(seed=0)
+    model.prep()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    X = torch.randn((N, SIDE, SIDE, 4), device="cuda", generator=g)
+    Y = torch.rand((train_batch, SIDE, SIDE), device="cuda", generator=g)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(warmup):
+        model.forward(X, dropout_seed=i + 1)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(steps):
+        model.forward(X, dropout_seed=i + 100)
+    e1.record()
+    e1.synchronize()
+    t_fwd = e0.elapsed_time(e1) / steps / 1e3
+    Xt = X[:train_batch].contiguous()
+    for i in range(warmup):
+        model.forward(Xt, dropout_seed=i + 1)
+        model.backward(Y)
+        model.adam(lr=1e-4)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(steps):
+        model.forward(Xt, dropout_seed=i + 100)
+        model.backward(Y)
+        model.adam(lr=1e-4)
+    e1.record()
+    e1.synchronize()
+    t_tr = e0.elapsed_time(e1) / steps / 1e3
+    if model.device_error():
+        raise RuntimeError("surrogate kernels reported a device error")
+    ff = model.flops_forward(N, SIDE, SIDE)
+    ft = 3.0 * model.flops_forward(train_batch, SIDE, SIDE)
+    return {"forward": {"images": N, "ms": t_fwd * 1e3, "tflops": ff / t_fwd / 1e12,
+                        "images_per_s": N / t_fwd},
+            "train_step": {"images": train_batch, "ms": t_tr * 1e3, "tflops": ft / t_tr / 1e12}}
+
+
+def conv_bench(N: int, H: int, Cin: int, Cout: int, steps: int = 5, warmup: int = 2) -> dict:
+    """Device time of one 3x3 convolution layer (forward) on N images of
+    H x H, random bf16 inputs."""
+    import torch
+    from .lib import core
+    from .unet import bordered
+    L = core()
+    x = bordered(N, H, H, Cin)
+    x.view(N, H + 2, H + 2, Cin)[:, 1:-1, 1:-1].normal_()
+    w = torch.randn((Cout, 9, Cin), device="cuda") / math.sqrt(9 * Cin)
+    wb = torch.empty((Cout, 9, Cin), dtype=torch.bfloat16, device="cuda")
+    wt = torch.empty((Cin, 9, Cout), dtype=torch.bfloat16, device="cuda")
+    L.fcab_unet_prep_weights(_ptr(w), _ptr(wb), _ptr(wt), Cout, Cin, None)
+    b = torch.zeros(Cout, device="cuda")
+    y = bordered(N, H, H, Cout)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(warmup):
+        L.fcab_unet_conv_fwd(_ptr(x), N, H, H, Cin, _ptr(wb), Cout, _ptr(b), 1, _ptr(y), None)
+    e0.record()
+    for _ in range(steps):
+        L.fcab_unet_conv_fwd(_ptr(x), N, H, H, Cin, _ptr(wb), Cout, _ptr(b), 1, _ptr(y), None)
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / steps / 1e3
+    flops = 2.0 * N * H * H * 9 * Cin * Cout
+    return {"conv": [N, H, Cin, Cout], "ms": t * 1e3, "tflops": flops / t / 1e12,
+            "error": L.fcab_unet_device_error()}
+
+
+def _ptr(t):
+    import ctypes as C
+    return C.c_void_p(t.data_ptr())
+
+
 def main(argv=None) -> int:
     import torch
     from .unet import UNet
     ap = argparse.ArgumentParser()
+    ap.add_argument("--conv-bench", default="",
+                    help="N,H,Cin,Cout: time one convolution layer only")
+    ap.add_argument("--layer-bench", action="store_true",
+                    help="time forward passes and training steps on random inputs only")
     ap.add_argument("--members", type=int, default=10000)
     ap.add_argument("--train", type=int, default=2000)
     ap.add_argument("--val", type=int, default=200)
@@ -205,6 +288,13 @@ def main(argv=None) -> int:
     ap.add_argument("--weights", default="", help="save the trained weights (.npz)")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
+    if a.layer_bench:
+        print(json.dumps(layer_bench()))
+        return 0
+    if a.conv_bench:
+        N, H, ci, co = (int(v) for v in a.conv_bench.split(","))
+        print(json.dumps(conv_bench(N, H, ci, co)))
+        return 0
     T = a.hours * 3600.0
     log = lambda r: print(json.dumps(r), flush=True)
     # training data from the CA

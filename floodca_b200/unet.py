@@ -4,7 +4,7 @@ Input channels: elevation relief, Manning n, rain intensity, rain duration
 (4 channels, stored in 16). Output: peak depth in a transformed scale.
 Encoder levels at 256/128/64/32 with 32/64/128/256 channels (two 3x3
 convolutions + ReLU each, 2x2 max pooling between); the decoder upsamples
-(nearest 2x), concatenates the skip connection and applies two 3x3
+(nearest 2x) and concatenates the skip connection in one pass, then applies two 3x3
 convolutions + ReLU; a 1x1 head gives one channel. Dropout (MC dropout at
 inference) follows the bottleneck and the two deeper decoder levels.
 
@@ -170,11 +170,8 @@ class UNet:
         for j, (ca, cb) in enumerate(self.dec):
             lvl = 2 - j
             skip, hs, ws, cs_ = skips[lvl]
-            up = self._buf(f"u{lvl}", N, hs, ws, cch)
-            check(L.fcab_unet_upsample2(_p(cur), _p(up), N, h, w, cch, st), "upsample")
             cat = self._buf(f"c{lvl}", N, hs, ws, cch + cs_)
-            check(L.fcab_unet_concat(_p(up), cch, _p(skip), cs_, _p(cat), N, hs, ws, 0, st),
-                  "concat")
+            check(L.fcab_unet_upcat(_p(cur), cch, _p(skip), cs_, _p(cat), N, hs, ws, st), "upcat")
             a = self._conv(ca, cat, N, hs, ws, f"d{lvl}a", st)
             b = self._conv(cb, a, N, hs, ws, f"d{lvl}b", st)
             acts[f"c{lvl}"], acts[f"d{lvl}a"], acts[f"d{lvl}b"] = cat, a, b
@@ -241,14 +238,11 @@ class UNet:
             gc = self._conv_bwd(ca, ga, A[f"c{lvl}"], A[f"d{lvl}a"], N, h, w, f"gc{lvl}", True, st)
             cup = ca.cin - self.enc[lvl][1].cout
             cs_ = self.enc[lvl][1].cout
-            gup = self._buf(f"gu{lvl}", N, h, w, cup)
-            gsk = self._buf(f"gs{lvl}", N, h, w, cs_)
-            check(L.fcab_unet_concat(_p(gup), cup, _p(gsk), cs_, _p(gc), N, h, w, 1, st),
-                  "concat_bwd")
-            skip_grads[lvl] = gsk
+            # the skip's share stays in gc until the pooling's backward adds it
+            skip_grads[lvl] = (gc, ca.cin, cup)
             hd, wd = sizes[lvl + 1]
             g = self._buf(f"gdn{lvl}", N, hd, wd, cup)
-            check(L.fcab_unet_upsample2_bwd(_p(gup), _p(g), N, hd, wd, cup, st), "upsample_bwd")
+            check(L.fcab_unet_upcat_bwd(_p(gc), cup, cs_, _p(g), N, h, w, st), "upcat_bwd")
         # encoder, bottleneck down to level 0
         for lvl in (3, 2, 1, 0):
             ca, cb = self.enc[lvl]
@@ -257,9 +251,9 @@ class UNet:
                 # gradient at e{lvl}b: through the pooling plus the skip
                 gb = self._buf(f"ge{lvl}b", N, h, w, cb.cout)
                 idx = self._idx(f"p{lvl}", N, h, w, cb.cout)
-                check(L.fcab_unet_maxpool2_bwd(_p(g), _p(idx), _p(gb), N, h, w, cb.cout, st),
-                      "maxpool_bwd")
-                check(L.fcab_unet_add(_p(gb), _p(skip_grads[lvl]), gb.numel(), st), "add")
+                gc, ctot, off = skip_grads[lvl]
+                check(L.fcab_unet_maxpool2_bwd_add(_p(g), _p(idx), _p(gc), ctot, off, _p(gb), N, h,
+                                                   w, cb.cout, st), "maxpool_bwd")
                 g = gb
             ds = (seed * 16 + 1) if (seed is not None and lvl == 3) else None
             xin = A["x0"] if lvl == 0 else A[f"p{lvl - 1}"]

@@ -393,6 +393,11 @@ FCAB_API int fcab_unet_maxpool2(const void *x, void *y, uint8_t *idx, int N, int
                                 void *stream);
 FCAB_API int fcab_unet_maxpool2_bwd(const void *dy, const uint8_t *idx, void *dx, int N, int H,
                                     int W, int C, void *stream);
+/* The same plus add[.][add_off .. add_off+C) (row width Cadd): the skip
+ * connection's share of a concatenation's gradient, added in one pass. */
+FCAB_API int fcab_unet_maxpool2_bwd_add(const void *dy, const uint8_t *idx, const void *add,
+                                        int Cadd, int add_off, void *dx, int N, int H, int W,
+                                        int C, void *stream);
 /* Nearest 2x upsampling of an (H, W) image; the backward sums 2x2 children. */
 FCAB_API int fcab_unet_upsample2(const void *x, void *y, int N, int H, int W, int C, void *stream);
 FCAB_API int fcab_unet_upsample2_bwd(const void *dy, void *dx, int N, int H, int W, int C,
@@ -400,6 +405,13 @@ FCAB_API int fcab_unet_upsample2_bwd(const void *dy, void *dx, int N, int H, int
 /* y = [a | b] along channels (backward != 0: split y into a and b). */
 FCAB_API int fcab_unet_concat(const void *a, int Ca, const void *b, int Cb, void *y, int N, int H,
                               int W, int backward, void *stream);
+/* y = [upsample2(coarse) | skip] for an (H, W) output in one pass, and the
+ * gradient of its upsampled part: gcoarse, an (H/2, W/2) image, sums the
+ * 2x2 children of gy[.][0..C1) (gy row width C1 + C2). */
+FCAB_API int fcab_unet_upcat(const void *coarse, int C1, const void *skip, int C2, void *y, int N,
+                             int H, int W, void *stream);
+FCAB_API int fcab_unet_upcat_bwd(const void *gy, int C1, int C2, void *gcoarse, int N, int H,
+                                 int W, void *stream);
 /* y += x, n bf16 elements. */
 FCAB_API int fcab_unet_add(void *y, const void *x, long long n, void *stream);
 /* g *= (y > 0), n elements. */
@@ -408,7 +420,7 @@ FCAB_API int fcab_unet_relu_bwd(void *g, const void *y, long long n, void *strea
 FCAB_API int fcab_unet_dropout(void *x, long long n, float p, uint32_t seed, void *stream);
 /* db[c] += sum over the P rows of g[.][C]. */
 FCAB_API int fcab_unet_bias_grad(const void *g, long long P, int C, float *db, void *stream);
-/* 1x1 output head C -> 1: out[N][H][W] fp32. */
+/* 1x1 output head C -> 1 (C = 32 or 64): out[N][H][W] fp32. */
 FCAB_API int fcab_unet_head_fwd(const void *x, const float *w, const float *b, float *out, int N,
                                 int H, int W, int C, void *stream);
 /* Mean squared error of out against target: dx (bf16), dw, db, loss sum

@@ -303,3 +303,37 @@ def test_unet_forward_backward_matches_torch():
         gb = b.grad.numpy()
         assert np.linalg.norm(gb - c.db.cpu().numpy()) <= 0.1 * np.linalg.norm(gb) + 1e-6
     assert np.allclose(model.dhw.cpu().numpy(), hw.grad.numpy(), rtol=0.05, atol=1e-4)
+
+
+def test_fused_upcat_and_pool_backward_add():
+    """upcat = concat(upsample2(coarse), skip); upcat_bwd = upsample2_bwd of
+    the first channels; maxpool2_bwd_add = maxpool2_bwd + a channel slice."""
+    L = core()
+    rng = np.random.default_rng(5)
+    N, H, W, C1, C2 = 2, 8, 12, 64, 32
+    co = _bf(rng.standard_normal((N, H // 2, W // 2, C1)))
+    sk = _bf(rng.standard_normal((N, H, W, C2)))
+    cob, skb = _to_b(co), _to_b(sk)
+    cat = torch.zeros((skb.shape[0], C1 + C2), dtype=torch.bfloat16, device="cuda")
+    assert L.fcab_unet_upcat(_p(cob), C1, _p(skb), C2, _p(cat), N, H, W, None) == 0
+    ref = np.concatenate([co.repeat(2, axis=1).repeat(2, axis=2), sk], -1)
+    assert np.array_equal(_from_b(cat, N, H, W)[:, 1:-1, 1:-1], ref)
+    g = _bf(rng.standard_normal((N, H, W, C1 + C2)))
+    gb = _to_b(g)
+    gco = torch.zeros_like(cob)
+    assert L.fcab_unet_upcat_bwd(_p(gb), C1, C2, _p(gco), N, H, W, None) == 0
+    s = g[..., :C1].reshape(N, H // 2, 2, W // 2, 2, C1).sum(axis=(2, 4))
+    assert np.allclose(_from_b(gco, N, H // 2, W // 2)[:, 1:-1, 1:-1], s, rtol=8e-3, atol=1e-2)
+    # pooling of the skip tensor and its gradient plus the concat slice
+    pooled = torch.zeros_like(cob[:, :C2].contiguous())
+    idx = torch.empty((N, H // 2, W // 2, C2), dtype=torch.uint8, device="cuda")
+    assert L.fcab_unet_maxpool2(_p(skb), _p(pooled), _p(idx), N, H, W, C2, None) == 0
+    dyp = _to_b(_bf(rng.standard_normal((N, H // 2, W // 2, C2))))
+    plain = torch.zeros_like(skb)
+    assert L.fcab_unet_maxpool2_bwd(_p(dyp), _p(idx), _p(plain), N, H, W, C2, None) == 0
+    fused = torch.zeros_like(skb)
+    assert L.fcab_unet_maxpool2_bwd_add(_p(dyp), _p(idx), _p(gb), C1 + C2, C1, _p(fused), N, H, W,
+                                        C2, None) == 0
+    want = _from_b(plain, N, H, W)[:, 1:-1, 1:-1] + g[..., C1:]
+    assert np.allclose(_from_b(fused, N, H, W)[:, 1:-1, 1:-1], want, rtol=8e-3, atol=1e-2)
+    assert _border_zero(fused, N, H, W) and _border_zero(cat, N, H, W)

@@ -171,7 +171,7 @@ def metrics(pred, truth, thr: float = 0.1) -> dict:
 
 
 def screen(model, X, passes: int = 8, area_thr_cells: int | None = None,
-           area_quantile: float = 0.9, spread_thr: float = 0.1) -> dict:
+           area_quantile: float = 0.9, spread_thr: float = 0.1, batch: int = 64) -> dict:
     """Surrogate pass over every member: per member the predicted area above
     0.3 m (cells) and the spread (mean over the predicted wet cells, > 0.1
     m, of the MC-dropout standard deviation). Returns the flags of members
@@ -179,7 +179,7 @@ def screen(model, X, passes: int = 8, area_thr_cells: int | None = None,
     import torch
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    mean, std = predict_mc(model, X, passes)
+    mean, std = predict_mc(model, X, passes, batch=batch)
     area = (mean > 0.3).flatten(1).sum(1)
     wet = (mean > 0.1).flatten(1)
     spread = (std.flatten(1) * wet).sum(1) / wet.sum(1).clamp_min(1)
@@ -190,6 +190,26 @@ def screen(model, X, passes: int = 8, area_thr_cells: int | None = None,
     rerun = (area > area_thr_cells) | (spread > spread_thr)
     return {"mean": mean, "rerun": rerun.cpu().numpy(), "area_thr_cells": area_thr_cells,
             "t_surrogate_s": t_sur, "spread": spread.cpu().numpy(), "area": area.cpu().numpy()}
+
+
+def screened_vs_plain(model, ms: list[Member], passes: int = 8, batch: int = 64) -> dict:
+    """The plain CA ensemble of ms and the surrogate-screened one: timings,
+    members/hour and the screened ensemble's accuracy against the CA."""
+    import torch
+    Yall, t_ca = run_ca(ms)
+    Xall = inputs(ms)
+    sc = screen(model, Xall, passes=passes, batch=batch)
+    rer = np.nonzero(sc["rerun"])[0]
+    Yre, t_re = run_ca([ms[i] for i in rer]) if len(rer) else (None, 0.0)
+    final = sc["mean"].clone()
+    if len(rer):
+        final[torch.as_tensor(rer, device="cuda")] = Yre
+    n = len(ms)
+    return {"plain_s": t_ca, "plain_members_per_hour": n / t_ca * 3600.0,
+            "surrogate_s": sc["t_surrogate_s"], "rerun_members": int(len(rer)), "rerun_s": t_re,
+            "screened_members_per_hour": n / (sc["t_surrogate_s"] + t_re) * 3600.0,
+            "accuracy": metrics(final, Yall), "surrogate_only": metrics(sc["mean"], Yall),
+            "area_thr_cells": sc["area_thr_cells"]}
 
 
 def layer_bench(N: int = 64, steps: int = 10, warmup: int = 3, train_batch: int = 32) -> dict:

@@ -25,6 +25,7 @@ struct Launchers {
     cudaError_t (*init)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl, int grid,
                         cudaStream_t s);
     const void *step_fn;   // __global__ symbol, for occupancy queries
+    int threads;           // threads per CTA of the step kernel
 };
 
 // Batched-ensemble launchers (FP32 state, FP64 accumulation).
@@ -62,7 +63,7 @@ template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool 
 cudaError_t launch_step(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
                         int warps_total, int grid, cudaStream_t s)
 {
-    k_step<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, 128, 0, s>>>(
+    k_step<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, step_threads<CPL, MATH>(), 0, s>>>(
         *static_cast<const GridD<T> *>(g), *static_cast<const RunK<T> *>(rk), tc, ctl,
         warps_total);
     return cudaGetLastError();
@@ -84,6 +85,7 @@ Launchers make_launchers()
     L.step = &launch_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
     L.init = &launch_init<T, K, MATH>;
     L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
+    L.threads = step_threads<CPL, MATH>();
     return L;
 }
 

@@ -217,14 +217,15 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     int dev = 0, nsm = 1, per_sm = 1;
     NA_TRY(cudaGetDevice(&dev));
     NA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    NA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.step_fn, 128, 0));
+    NA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.step_fn, L.threads, 0));
+    const int wpb = L.threads / 32;
     const int ow = 32 * key.cpl - 2 * (key.cpl == 1 ? 3 : 4);
     const long long total = ((cfg->ncols + ow - 1) / ow) * (long long)cfg->nrows;
     long long warps = (total + 47) / 48;
-    const long long maxw = (long long)nsm * (per_sm > 0 ? per_sm : 1) * 4;
+    const long long maxw = (long long)nsm * (per_sm > 0 ? per_sm : 1) * wpb;
     warps = warps < maxw ? warps : maxw;
     warps = warps < 1 ? 1 : warps;
-    const int grid = (int)((warps + 3) / 4);
+    const int grid = (int)((warps + wpb - 1) / wpb);
 
     if (stats) {   // V0, the LAND volume of the initial depth
         NA_TRY(cudaMemsetAsync(vol, 0, 2 * sizeof(double), s));
@@ -233,7 +234,7 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     }
     NA_TRY(L.init(&g, &rk, tc, ctl, nsm * 4, s));
     for (int k = 0; k < cfg->max_steps; k++)
-        NA_TRY(L.step(&g, &rk, tc, ctl, grid * 4, grid, s));
+        NA_TRY(L.step(&g, &rk, tc, ctl, grid * wpb, grid, s));
     k_unpack<<<512, 256, 0, s>>>(g, ctl, h, hmax, tmax);
     NA_TRY(cudaGetLastError());
 

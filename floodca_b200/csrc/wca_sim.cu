@@ -512,7 +512,7 @@ static int resolve_variant(FcabSim *s)
     // Grid: resident CTAs, or fewer so every warp streams >= seg_rows rows.
     int nsm = 0, per_sm = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->dev));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->L.step_fn, 128, 0));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->L.step_fn, s->L.threads, 0));
     if (per_sm < 1)
         per_sm = 1;
     const int ow = 32 * s->cpl - 2 * (s->cpl == 1 ? 3 : 4);
@@ -520,12 +520,13 @@ static int resolve_variant(FcabSim *s)
     const long long total = strips * s->cfg.nrows;
     const int seg = s->cfg.seg_rows > 0 ? s->cfg.seg_rows : 48;
     long long want_warps = (total + seg - 1) / seg;
-    long long max_warps = (long long)nsm * per_sm * 4;
+    const int wpb = s->L.threads / 32;     // warps per CTA
+    long long max_warps = (long long)nsm * per_sm * wpb;
     long long warps = want_warps < max_warps ? want_warps : max_warps;
     if (warps < 1)
         warps = 1;
-    s->grid = (int)((warps + 3) / 4);
-    s->warps_total = s->grid * 4;
+    s->grid = (int)((warps + wpb - 1) / wpb);
+    s->warps_total = s->grid * wpb;
     s->occupancy = per_sm;
     if (s->graph) {
         cudaGraphExecDestroy(s->graph);

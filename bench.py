@@ -43,12 +43,8 @@ BYTES_PER_CELL = 25  # read z, h, n, hmax (4 B each) + mask (1 B); write h, hmax
 
 
 def warm_domain(n: int):
-    from floodca_b200 import synth
-    dom, p = synth.config2(n=n)
-    dom = dom.copy()
-    dom.h = np.full(dom.shape, 0.02, np.float32)
-    dom.hmax = dom.h.copy()
-    return dom, p
+    from floodca_b200.profile_step import warm_config2
+    return warm_config2(n)
 
 
 def measured_peaks() -> dict:

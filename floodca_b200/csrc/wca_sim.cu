@@ -894,7 +894,8 @@ __global__ void k_count(GridD<T> g, int nthr, double t0, double t1, double t2, d
             mx = hm;
         for (int j = 0; j < nthr; j++) {
             if ((double)hm >= thr[j]) {
-                counts[(long long)j * N + i]++;
+                if (counts)
+                    counts[(long long)j * N + i]++;
                 f[j]++;
             }
         }

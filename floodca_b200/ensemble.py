@@ -174,9 +174,49 @@ def seg_for(side: int, tuning: dict) -> int:
     return 64
 
 
+THRESHOLDS = (0.10, 0.25, 0.50)
+ROW_FIELDS = ("member", "side", "seed", "n_scale", "rain_mm_h", "rain_h", "rank", "steps",
+              "sim_time_s", "rain_volume_m3", "boundary_volume_m3", "mass_err_rel",
+              "flooded_cells_010", "flooded_cells_025", "flooded_cells_050", "max_depth_m")
+
+
+def member_row(idx: int, m: Member, s: Session, rank: int = 0) -> dict:
+    """One member's summary in the layout of the reference ensemble's
+    per-scenario CSV (src/hybrid/ens_common.c:223-258): steps, simulated
+    time, rain volume, mass-balance error, flooded cells at 0.10 / 0.25 /
+    0.50 m and the largest peak depth."""
+    st = s.stats()
+    fl, mx = s.count_flooded(THRESHOLDS)
+    return {"member": idx, "side": m.side, "seed": m.seed, "n_scale": m.n_scale,
+            "rain_mm_h": m.rain_mm_h, "rain_h": m.rain_h, "rank": rank, "steps": st["step"],
+            "sim_time_s": st["t"], "rain_volume_m3": st["V_rain"],
+            "boundary_volume_m3": st["V_bnd"], "mass_err_rel": st["E_mass"],
+            "flooded_cells_010": fl[0], "flooded_cells_025": fl[1], "flooded_cells_050": fl[2],
+            "max_depth_m": mx}
+
+
+def write_rows(path, rows: list[dict]) -> None:
+    with open(path, "w") as f:
+        f.write(",".join(ROW_FIELDS) + "\n")
+        for r in sorted(rows, key=lambda r: r["member"]):
+            f.write(",".join(str(r[k]) for k in ROW_FIELDS) + "\n")
+
+
+def gather_rows(rows: list[dict]) -> list[dict]:
+    """Every rank's member rows, on every rank (one host gather after the
+    run: the only collective of the sharded ensemble)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(rows)
+    out = [None] * dist.get_world_size()
+    dist.all_gather_object(out, list(rows))
+    return sorted((r for part in out for r in part), key=lambda r: r["member"])
+
+
 def run_batched(members: list[Member], math="exact", tuning: dict | None = None,
-                window=0.0, graph_steps=16, collect=False) -> dict:
-    """All members in one batch; window > 0 paces them by output windows."""
+                window=0.0, graph_steps=16, collect=False, ids=None, rank: int = 0) -> dict:
+    """All members in one batch; window > 0 paces them by output windows.
+    ids: the members' indices in the whole ensemble (for the rows)."""
     tuning = tuning or DEFAULT_TUNING
     t0 = time.perf_counter()
     sessions = [member_session(m, math) for m in members]
@@ -189,10 +229,12 @@ def run_batched(members: list[Member], math="exact", tuning: dict | None = None,
     _sync()
     wall = time.perf_counter() - t1
     stats = [s.stats() for s in sessions]
+    ids = list(range(len(members))) if ids is None else list(ids)
     out = {"members": len(members), "wall_s": wall, "setup_s": t_setup,
            "members_per_hour": len(members) / wall * 3600.0, "info": b.info(),
            "cell_steps": sum(st["step"] * m.side * m.side for st, m in zip(stats, members)),
-           "stats": stats}
+           "stats": stats,
+           "rows": [member_row(i, m, s, rank) for i, m, s in zip(ids, members, sessions)]}
     if collect:
         out["hmax"] = [s.download()[1] for s in sessions]
     b.close()
@@ -344,6 +386,7 @@ def main(argv=None) -> int:
     ap.add_argument("--retune", action="store_true")
     ap.add_argument("--paced", action="store_true", help="also time the 10-minute paced run")
     ap.add_argument("--out", default="")
+    ap.add_argument("--csv", default="", help="per-member rows (rank 0 writes all ranks')")
     a = ap.parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -358,8 +401,9 @@ def main(argv=None) -> int:
     tune = DEFAULT_TUNING if a.no_tune else autotune(members, a.math,
                                                      cache=Path(a.tuning_cache),
                                                      force=a.retune)
-    bat = run_batched(local, a.math, tune, window=0.0)
+    bat = run_batched(local, a.math, tune, window=0.0, ids=mine, rank=rank)
     wall = bat["wall_s"]
+    rows = gather_rows(bat["rows"])
     if world > 1:
         import torch
         import torch.distributed as dist
@@ -379,6 +423,9 @@ def main(argv=None) -> int:
                        "gcell_steps_per_s": total_cells / wall / 1e9,
                        "setup_s_rank0": bat["setup_s"], "info_rank0": bat["info"]}}
     if rank == 0:
+        res["members_rows"] = len(rows)
+        if a.csv:
+            write_rows(a.csv, rows)
         if a.paced:
             paced = run_batched(local, a.math, tune, window=600.0)
             res["batched_paced_600s_rank0"] = {

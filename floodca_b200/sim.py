@@ -188,6 +188,19 @@ class Session:
               "fcab_sim_download")
         return h, hmax, tmax
 
+    def count_flooded(self, thresholds=(0.10, 0.25, 0.50), counts=None):
+        """LAND cells with hmax >= each threshold and the largest LAND hmax;
+        counts: optional device uint16 raster [len(thresholds), rows, cols]
+        (a torch tensor) that the flooded cells are added into."""
+        n = len(thresholds)
+        thr = (C.c_double * n)(*thresholds)
+        fl = (C.c_longlong * n)()
+        mx = C.c_double()
+        cp = None if counts is None else C.c_void_p(counts.data_ptr())
+        check(self.L.fcab_sim_count_flooded(self.h, n, thr, cp, fl, C.byref(mx)),
+              "fcab_sim_count_flooded")
+        return [int(v) for v in fl], float(mx.value)
+
     def launches(self) -> int:
         return int(self.L.fcab_sim_launches(self.h))
 

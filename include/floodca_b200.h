@@ -273,8 +273,8 @@ FCAB_API int fcab_sim_set_pause_every(FcabSim *s, int nsteps, int n_force_days);
 FCAB_API int fcab_sim_upload_state(FcabSim *s, const void *h, const void *hmax, const void *tmax);
 
 /* Adds hmax >= thr[j] on LAND cells into the device array counts[j*N + a]
- * (uint16, N = nrows*ncols, at most 4 thresholds) and returns the flooded
- * cell counts and the largest LAND hmax (at least 0). */
+ * (uint16, N = nrows*ncols, at most 4 thresholds; NULL: no raster) and
+ * returns the flooded cell counts and the largest LAND hmax (at least 0). */
 FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uint16_t *counts,
                            long long *flooded, double *max_depth);
 

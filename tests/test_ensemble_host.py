@@ -65,18 +65,21 @@ def _gloo_rank(rank, world, port, q):
     from floodca_b200.ensemble import config4_members as mk, shard
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
+    from floodca_b200.ensemble import gather_rows
     mine = shard(mk(64), rank, world)
     got = [None] * world
     dist.all_gather_object(got, mine)
     t = torch.tensor([float(len(mine))])
     dist.all_reduce(t)
-    q.put((rank, got, float(t)))
+    rows = gather_rows([{"member": i, "rank": rank, "steps": 10 + i} for i in mine])
+    q.put((rank, got, float(t), rows))
     dist.destroy_process_group()
 
 
 def test_shard_gloo_two_ranks():
     """Two ranks compute their shards independently; together they cover
-    every member once (what the torchrun ensemble relies on)."""
+    every member once, and the one host gather after the run gives every
+    rank all member rows (what the torchrun ensemble relies on)."""
     import multiprocessing as mp
     import socket
     with socket.socket() as s:
@@ -91,9 +94,13 @@ def test_shard_gloo_two_ranks():
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, got, total in res:
+    for rank, got, total, rows in res:
         assert sorted(got[0] + got[1]) == list(range(64)) and not set(got[0]) & set(got[1])
         assert total == 64.0
+        # every rank holds every member's row once, from the rank that ran it
+        assert [r["member"] for r in rows] == list(range(64))
+        owner = {i: k for k in range(2) for i in got[k]}
+        assert all(r["rank"] == owner[r["member"]] and r["steps"] == 10 + r["member"] for r in rows)
 
 
 def test_choose_tuning():
@@ -110,3 +117,13 @@ def test_choose_tuning():
     assert t["seg_rows_by_class"] == [[0, 1023, 32], [1536, 1 << 30, 64]]
     from floodca_b200.ensemble import seg_for
     assert seg_for(512, t) == 32 and seg_for(2048, t) == 64 and seg_for(1100, t) == 64
+
+
+def test_write_rows(tmp_path):
+    from floodca_b200.ensemble import ROW_FIELDS, write_rows
+    rows = [{k: (i if k == "member" else 0.5) for k in ROW_FIELDS} for i in (2, 0, 1)]
+    p = tmp_path / "m.csv"
+    write_rows(p, rows)
+    lines = p.read_text().splitlines()
+    assert lines[0].split(",") == list(ROW_FIELDS)
+    assert [ln.split(",")[0] for ln in lines[1:]] == ["0", "1", "2"]

@@ -132,3 +132,19 @@ def test_device_members_equal_host_members():
         _check_equal(single, s)
     finally:
         s.close()
+
+
+def test_member_rows_match_downloaded_depths():
+    """The per-member rows (reference ensemble CSV layout) agree with each
+    member's downloaded peak depth."""
+    from floodca_b200.ensemble import THRESHOLDS, run_batched
+    ms = [Member(side=128, seed=31 + i, n_scale=1.0, rain_mm_h=60.0 + 40 * i, rain_h=1.0,
+                 T_sim=3600.0) for i in range(3)]
+    out = run_batched(ms, collect=True, ids=[7, 8, 9])
+    for row, hm, st in zip(out["rows"], out["hmax"], out["stats"]):
+        assert row["steps"] == st["step"] and row["sim_time_s"] == st["t"]
+        for t, key in zip(THRESHOLDS, ("flooded_cells_010", "flooded_cells_025",
+                                       "flooded_cells_050")):
+            assert row[key] == int((hm.astype(np.float64) >= t).sum())
+        assert row["max_depth_m"] == pytest.approx(float(hm.max()), rel=1e-7)
+    assert [r["member"] for r in out["rows"]] == [7, 8, 9]

@@ -175,6 +175,103 @@ def config_block(n: int, gpus: int) -> dict:
             "l2": "inputs (~420 MB per step) larger than L2; no flush"}
 
 
+def e2e_mass_error(r: dict) -> float:
+    """|V + V_sea + V_bnd - V_rain - V0 - clamp| / (V_rain + V0) of a run
+    through the drop-in ABI (the reference's diag.c:5-14)."""
+    den = max(r["V_rain"] + r["V0"], 1e-30)
+    return abs(r["V"] + r["V_sea"] + r["V_bnd"] - r["V_rain"] - r["V0"] - r["clamp_err"]) / den
+
+
+# ---------------------------------------------------------------------------
+# Per-configuration table: the same workloads on the GPU (sessions) and on the
+# reference's OpenMP core with all host threads and with one.
+
+TABLE_CONFIGS = {
+    "C1": "config 1, 256x256, full run (2 h simulated)",
+    "C2": "config 2, 4096x4096, warm, fixed step window",
+    "C3": "config 3, 2048x2048, warm, fixed step window",
+}
+
+
+def _table_domain(name: str):
+    from floodca_b200 import synth
+    if name == "C1":
+        return synth.config1()
+    if name == "C2":
+        return warm_domain(4096)
+    dom, p = synth.config3()
+    dom = dom.copy()
+    dom.h = np.full(dom.shape, 0.02, np.float32)
+    dom.hmax = dom.h.copy()
+    return dom, p
+
+
+def cpu_table_worker(name: str, steps: int) -> dict:
+    """Runs in a child process so OMP_NUM_THREADS takes effect."""
+    from oracle import refcore
+    kind = refcore.shipped_kind()
+    if not refcore.available(kind):
+        return {"unavailable": "reference not built"}
+    dom, p = _table_domain(name)
+    cells = int((dom.mask == 0).sum())
+    if name == "C1":
+        t0 = time.perf_counter()
+        r = refcore.run(dom, p, kind)
+        wall = time.perf_counter() - t0
+        return {"gcells": cells * r["step"] / wall / 1e9, "steps": r["step"], "wall_s": wall}
+    run = refcore.RefRun(dom, p.with_(steps=0, T_sim=1e7), kind)
+    run.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run.step()
+    wall = time.perf_counter() - t0
+    return {"gcells": cells * steps / wall / 1e9, "steps": steps, "wall_s": wall}
+
+
+def config_table() -> dict:
+    import torch
+    from floodca_b200.sim import Session
+    cores = os.cpu_count() or 1
+    out = {"cores": cores, "rows": []}
+    for name, desc in TABLE_CONFIGS.items():
+        dom, p = _table_domain(name)
+        land = int((dom.mask == 0).sum())
+        s = Session(dom, p if name == "C1" else p.with_(T_sim=30 * 86400.0))
+        st = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if name == "C1":
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.run()
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            steps = s.stats()["step"]
+            gpu = land * steps / wall / 1e9
+        else:
+            s.advance(20)
+            torch.cuda.synchronize()
+            e0.record(st)
+            s.advance(200)
+            e1.record(st)
+            e1.synchronize()
+            steps = 200
+            gpu = land * steps / (e0.elapsed_time(e1) / 1e3) / 1e9
+        s.close()
+        row = {"config": name, "workload": desc, "land_cells": land, "gpu_gcells": gpu,
+               "gpu_timing": "host wall, whole run" if name == "C1" else "CUDA events, 200 steps"}
+        for label, threads, k in (("cpu_omp", cores, 10), ("cpu_1thread", 1, 3)):
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close",
+                       OMP_PLACES="cores")
+            r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--cpu-worker", name,
+                                str(k)], capture_output=True, text=True, env=env, timeout=900)
+            try:
+                row[label] = json.loads(r.stdout.strip().splitlines()[-1])
+            except (IndexError, ValueError):
+                row[label] = {"unavailable": r.stderr[-300:]}
+        out["rows"].append(row)
+    return out
+
+
 # ---------------------------------------------------------------------------
 
 def main() -> int:
@@ -190,7 +287,16 @@ def main() -> int:
                     help="seconds of CPU time for the reference baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--config-table", action="store_true",
+                    help="GPU vs reference CPU (all threads, one thread) on configs 1-3")
+    ap.add_argument("--cpu-worker", nargs=2, metavar=("CONFIG", "STEPS"), help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_worker:
+        print(json.dumps(cpu_table_worker(args.cpu_worker[0], int(args.cpu_worker[1]))))
+        return 0
+    if args.config_table:
+        print(json.dumps(config_table(), indent=1))
+        return 0
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -279,8 +385,10 @@ def main() -> int:
         out["e2e"] = {"value": world * land * steps / wall / 1e9, "unit": "Gcell/s",
                       "h2d_bytes_per_step": es * n * n / max(steps, 1),
                       "d2h_bytes_per_step": 12 * n * n / max(steps, 1),
-                      "api": "fca_cuda_run (host buffers)", "run": "config 2, 6 h simulated",
-                      "steps": steps, "wall_s": wall, "rc": rc, "E_mass": None}
+                      "api": "fca_cuda_run (host buffers)",
+                      "run": "config 2, 6 h simulated, without the point inflow (the reference "
+                             "ABI has no inflow term)",
+                      "steps": steps, "wall_s": wall, "rc": rc, "E_mass": e2e_mass_error(res)}
     if rank == 0 and world == 1 and not args.no_cpu:
         r = reference_cpu(dom, p, 5, 1, args.cpu_budget)
         if "unavailable" not in r:

@@ -195,7 +195,11 @@ static int pick_cpl(const FcabConfig &c)
 {
     if (c.cols_per_lane == 1 || c.cols_per_lane == 2 || c.cols_per_lane == 4)
         return c.cols_per_lane;
-    if (c.ncols <= 64)
+    // 1-column lanes for grids too small to fill the GPU with 2-column
+    // strips (measured on a B200: CPL 1 is faster up to 1024^2, CPL 2 from
+    // 2048^2 on, where its smaller halo share wins)
+    const long long strips2 = (c.ncols + 55) / 56;
+    if (c.ncols <= 64 || strips2 * c.nrows < 40960)
         return 1;
     return 2;
 }
@@ -518,10 +522,14 @@ static int resolve_variant(FcabSim *s)
     const int ow = 32 * s->cpl - 2 * (s->cpl == 1 ? 3 : 4);
     const long long strips = (s->cfg.ncols + ow - 1) / ow;
     const long long total = strips * s->cfg.nrows;
-    const int seg = s->cfg.seg_rows > 0 ? s->cfg.seg_rows : 48;
-    long long want_warps = (total + seg - 1) / seg;
     const int wpb = s->L.threads / 32;     // warps per CTA
     long long max_warps = (long long)nsm * per_sm * wpb;
+    // rows per warp: enough warps to fill the resident slots, but at least 4
+    // rows per warp (each warp's segment costs 6 extra pipeline rows)
+    long long seg = s->cfg.seg_rows > 0 ? s->cfg.seg_rows : total / max_warps;
+    if (seg < 4)
+        seg = 4;
+    long long want_warps = (total + seg - 1) / seg;
     long long warps = want_warps < max_warps ? want_warps : max_warps;
     if (warps < 1)
         warps = 1;

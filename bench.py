@@ -368,6 +368,9 @@ def main() -> int:
 
     if not args.no_e2e:
         dom2, p2 = __import__("floodca_b200.synth", fromlist=["config2"]).config2(n=n)
+        # one untimed run first (one-time costs of the process: module
+        # loading, first allocations), then the timed run
+        DropinGrid(dom2, p2.with_(steps=20)).run()
         g = DropinGrid(dom2, p2)
         torch.cuda.synchronize()
         if world > 1:
@@ -388,7 +391,8 @@ def main() -> int:
                       "api": "fca_cuda_run (host buffers)",
                       "run": "config 2, 6 h simulated, without the point inflow (the reference "
                              "ABI has no inflow term)",
-                      "steps": steps, "wall_s": wall, "rc": rc, "E_mass": e2e_mass_error(res)}
+                      "steps": steps, "wall_s": wall, "rc": rc, "E_mass": e2e_mass_error(res),
+                      "t_h2d_s": g.tm.t_h2d, "t_d2h_s": g.tm.t_d2h}
     if rank == 0 and world == 1 and not args.no_cpu:
         r = reference_cpu(dom, p, 5, 1, args.cpu_budget)
         if "unavailable" not in r:

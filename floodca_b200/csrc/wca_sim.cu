@@ -431,11 +431,24 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
         mh = probe.data();
     }
     const int has_sea = memchr(mh, M_SEA, (size_t)N) != nullptr;
+    // LAND cells per row; open faces only on the open edges' rows/columns
+    s->land_cells = 0;
+    s->open_faces = 0;
+    const bool open = c.boundary == FCA_BND_OPEN;
+    for (long long r = 0; r < c.nrows; r++) {
+        const uint8_t *row = mh + r * c.ncols;
+        long long cnt = 0;
+        for (long long k = 0; k < c.ncols; k++)
+            cnt += row[k] == M_LAND;
+        s->land_cells += cnt;
+        if (open) {
+            s->open_faces += (r == 0 && c.edge_n ? cnt : 0) + (r == c.nrows - 1 && c.edge_s ? cnt : 0);
+            s->open_faces += (c.edge_w && row[0] == M_LAND) + (c.edge_e && row[c.ncols - 1] == M_LAND);
+        }
+    }
     // all-LAND grids use the mask-free kernel: padding elevation PAD_Z makes
     // every face to the padding carry zero discharge (needs tau_h > 0)
-    bool all_land = c.tau_h > 0.0;
-    for (long long i = 0; i < N && all_land; i++)
-        all_land = mh[i] == M_LAND;
+    const bool all_land = c.tau_h > 0.0 && s->land_cells == N;
     s->landonly = all_land;
     if (all_land) {
         k_fill_all<<<1024, 256, 0, s->stream>>>(s->z, (long long)s->nelem, PAD_Z, (int)es);
@@ -445,18 +458,6 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
     int inflow_ok = 0;
     if (c.inflow_cell >= 0 && c.inflow_cell < N)
         inflow_ok = mh[c.inflow_cell] == M_LAND;
-    s->land_cells = 0;
-    s->open_faces = 0;
-    for (long long i = 0; i < N; i++) {
-        if (mh[i] != M_LAND)
-            continue;
-        s->land_cells++;
-        if (c.boundary == FCA_BND_OPEN) {
-            const int r = (int)(i / c.ncols), cc = (int)(i % c.ncols);
-            s->open_faces += (cc == 0 && c.edge_w) + (cc == c.ncols - 1 && c.edge_e) +
-                             (r == 0 && c.edge_n) + (r == c.nrows - 1 && c.edge_s);
-        }
-    }
     const long long nr = c.nrows, nc = c.ncols;
     s->faces_per_step = nr * (nc - 1) + (nr - 1) * nc +
                         (c.K == 8 ? 2 * (nr - 1) * (nc - 1) : 0) + s->open_faces;

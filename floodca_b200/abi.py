@@ -124,7 +124,7 @@ class FcabStats(C.Structure):
         ("V", C.c_double), ("V0", C.c_double), ("V_rain", C.c_double), ("V_sea", C.c_double),
         ("V_bnd", C.c_double), ("clamp_err", C.c_double), ("V_in", C.c_double),
         ("cap_active", C.c_longlong), ("cap_total", C.c_longlong), ("dt_min_hits", C.c_longlong),
-        ("E_mass", C.c_double),
+        ("E_mass", C.c_double), ("dt_full_passes", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:

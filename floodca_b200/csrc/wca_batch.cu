@@ -111,6 +111,7 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
         d.g.nc = s->cfg.ncols;
         d.rk = s->rkf;
         d.tc = s->tc;
+        d.tc.vseed_on = 0;    // batches prune without a seed (no full pass between steps)
         d.ctl = s->ctl;
         d.strips = (s->cfg.ncols + ow - 1) / ow;
         d.seg = member_seg_rows && member_seg_rows[i] > 0 ? member_seg_rows[i] : b->seg;

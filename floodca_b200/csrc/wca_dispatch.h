@@ -22,8 +22,11 @@ struct VariantKey {
 struct Launchers {
     cudaError_t (*step)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
                         int warps_total, int grid, cudaStream_t s);
+    // full velocity pass + step control: the first step's dt, or
+    // (only_if_needed) a dt deferred by a step whose pruned maximum fell
+    // below its seed
     cudaError_t (*init)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl, int grid,
-                        cudaStream_t s);
+                        cudaStream_t s, int only_if_needed);
     const void *step_fn;   // __global__ symbol, for occupancy queries
     int threads;           // threads per CTA of the step kernel
 };
@@ -71,10 +74,11 @@ cudaError_t launch_step(const void *g, const void *rk, const TimeCfg &tc, Ctl *c
 
 template <typename T, int K, int MATH>
 cudaError_t launch_init(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl, int grid,
-                        cudaStream_t s)
+                        cudaStream_t s, int only_if_needed)
 {
     k_init_dt<T, K, MATH><<<grid, 256, 0, s>>>(*static_cast<const GridD<T> *>(g),
-                                              *static_cast<const RunK<T> *>(rk), tc, ctl);
+                                              *static_cast<const RunK<T> *>(rk), tc, ctl,
+                                              only_if_needed);
     return cudaGetLastError();
 }
 

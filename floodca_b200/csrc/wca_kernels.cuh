@@ -69,6 +69,12 @@ struct RunK {
     int has_sea;
 };
 
+// Fraction of a step's velocity maximum that seeds the next step's dt
+// pruning.
+#ifndef FCAB_VSEED_FRAC
+#define FCAB_VSEED_FRAC 0.9
+#endif
+
 // Host-visible control block; one per run, in device memory.
 struct Ctl {
     // prepared for the next step by the previous step's last CTA
@@ -82,6 +88,12 @@ struct Ctl {
     double window_end;          // > 0: pause once t reaches it (batched ensembles)
     double V_in;                // inflow volume added by the steps taken
     double V_in_step;           // inflow volume of the prepared step
+    // velocity seed of the next step's dt pruning (float or double bits, 0:
+    // none) and the deferred-dt handshake with the full velocity pass
+    unsigned long long vseed_bits;
+    int need_v;                 // the step's pruned maximum fell below the seed
+    int pause_carry;            // progress pause decided before the deferral
+    long long full_passes;      // deferred dts completed by the full pass
     double accd[4][NSLOT];      // V_rain, clamp, V_sea, V_bnd (double accumulation)
     float accf[4][NSLOT];       // same, FP32 accumulation
     unsigned long long cap[NSLOT];
@@ -94,6 +106,8 @@ struct TimeCfg {
     double alpha_dx_d;
     int hyeto, max_steps, U, time_f32;
     int n_force_days, progress_every, inflow_ok, prec_f64;
+    int vseed_on;               // seed the dt pruning (the launcher adds the full pass)
+    int pad_tc;
 };
 
 // --------------------------------------------------------------------------
@@ -209,6 +223,8 @@ __device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool afte
     }
     if (!done && after_step && tc.progress_every > 0 && step % tc.progress_every == 0)
         pause = 1;
+    if (!done && c->pause_carry)
+        pause = 1;                  // decided before a deferred dt
     if (!done && c->window_end > 0.0 && t >= c->window_end - 1e-9)
         pause = 1;                  // end of an output window
     T dt_base = (T)c->dt_base;
@@ -218,6 +234,36 @@ __device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool afte
             vmax = (T)__uint_as_float((unsigned)c->vmax_bits);
         else
             vmax = (T)__longlong_as_double((long long)c->vmax_bits);
+        T seed;
+        if (sizeof(T) == 4)
+            seed = (T)__uint_as_float((unsigned)c->vseed_bits);
+        else
+            seed = (T)__longlong_as_double((long long)c->vseed_bits);
+        if (after_step && tc.vseed_on && vmax < seed) {
+            c->full_passes += 1;
+            // cells pruned against the seed may hold the maximum: keep the
+            // time advance, defer dt to the full velocity pass (k_init_dt)
+            c->t = t;
+            c->step = step;
+            c->pause_carry = pause;
+            c->need_v = 1;
+            c->active = 0;
+            c->vmax_bits = 0ull;
+            c->ctas_done = 0u;
+            return;
+        }
+        // seed of the next dt computation: pruning against FCAB_VSEED_FRAC of this
+        // step's maximum; a step whose maximum falls below it is redone
+        // by the full pass
+        if (tc.vseed_on) {
+            const T sd = vmax * T(FCAB_VSEED_FRAC);
+            if (sizeof(T) == 4)
+                c->vseed_bits = (unsigned long long)__float_as_uint((float)sd);
+            else
+                c->vseed_bits = (unsigned long long)__double_as_longlong((double)sd);
+        } else {
+            c->vseed_bits = 0ull;
+        }
         T dtm = rk.dt_max;
         if (vmax > T(0)) {
             T dta = rk.k.alpha_dx / vmax;
@@ -267,6 +313,8 @@ __device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool afte
     else
         c->tmax_val = t + (double)dt;
     c->want_v = (step + 1) % tc.U == 0;
+    c->need_v = 0;
+    c->pause_carry = 0;
     c->done = done ? 1 : 0;
     c->pause = pause;
     c->active = (!done && !pause) ? 1 : 0;
@@ -468,6 +516,7 @@ template <typename T>
 struct StepVals {
     StepK<T> k;
     T dt, A, F, tmax_val, inflow_dh, rainv, dd, qnan;
+    T vseed;                     // prune dt candidates below this velocity (0: none)
     int want_v;
     const T *hin;
     T *hout;
@@ -475,7 +524,7 @@ struct StepVals {
 
 template <typename T, int K>
 __device__ __forceinline__ StepVals<T> step_vals(const GridD<T> &g, const RunK<T> &rk,
-                                                const Ctl *ctl)
+                                                const Ctl *ctl, bool use_seed = true)
 {
     StepVals<T> v;
     v.k = rk.k;
@@ -493,6 +542,14 @@ __device__ __forceinline__ StepVals<T> step_vals(const GridD<T> &g, const RunK<T
     v.rainv = rk.cr_uniform * v.F;   // C*Rday*F for a uniform field
     v.dd = v.k.d_diag;
     v.qnan = qnan_of<T>();
+    if (use_seed) {
+        if constexpr (sizeof(T) == 4)
+            v.vseed = (T)__uint_as_float((unsigned)ctl->vseed_bits);
+        else
+            v.vseed = (T)__longlong_as_double((long long)ctl->vseed_bits);
+    } else {
+        v.vseed = T(0);
+    }
     return v;
 }
 
@@ -518,7 +575,7 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
     using G = Geom<CPL>;
     const StepK<T> &k = sv.k;
     const T dt = sv.dt, A = sv.A, F = sv.F, tmax_val = sv.tmax_val, inflow_dh = sv.inflow_dh;
-    const T rainv = sv.rainv, dd = sv.dd, qnan = sv.qnan;
+    const T rainv = sv.rainv, dd = sv.dd, qnan = sv.qnan, vseed = sv.vseed;
     const int want_v = sv.want_v;
     const T *hin = sv.hin;
     T *hout = sv.hout;
@@ -753,7 +810,8 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
                                                          (r == nr - 1 && rk.edge_s)));
             const bool row2_in = r >= 0 && r < nr;
             // stage-E threshold: the warp's running velocity maximum
-            const T thr = want_v ? warp_max_nonneg(vmax) : T(0);
+            T thr = want_v ? warp_max_nonneg(vmax) : T(0);
+            thr = thr > vseed ? thr : vseed;
             T *tm_row = g.tmax + (long long)(r + PADR) * g.pitch + colo;
             bool rose_any = false, bnd_open = false;
             T qbnd[CPL];
@@ -867,8 +925,13 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
                     hn2[j] = ha;
                     Ln2[j] = ma == M_WALL ? qnan : (ma == M_SEA ? k.z_sea : p2.z[j] + ha);
                 }
+                // prefilter of the next dt: a cell whose critical velocity
+                // sqrt(g h) is surely below thr cannot raise the maximum
+                // (g h <= thr^2 (1 - 1e-6): the margin covers the rounding of
+                // both products and of the square root by far); flagged
+                // cells get the exact evaluation in stage E
                 if (want_v && cell_out && land && ha >= k.tau_h &&
-                    !(thr > T(0) && Mth<T, MATH>::vcr_le(thr, k.g, ha)))
+                    !(thr > T(0) && k.g * ha <= thr * thr * T(0.999999)))
                     eflag_next |= 1u << j;
                 const bool rise = cell_out && land && ha > hm[j];
                 hmx[j] = rise ? ha : hm[j];
@@ -938,7 +1001,8 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
                     const T sd = md * k.rdd;
                     Sb = sd > Sb ? sd : Sb;
                 }
-                if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <= vmax)
+                if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <=
+                    (vmax > vseed ? vmax : vseed))
                     continue;
                 T Smax = Mth<T, MATH>::div(mo, k.dx);
                 if constexpr (K == 8) {
@@ -1141,7 +1205,7 @@ k_step_batch(const MemberD<T> *members,
         const int local = (int)u - md.unit_off;
         const int strip = local % md.strips, blk = local / md.strips;
         const int r0 = blk * md.seg, r1 = min(g.nr, r0 + md.seg);
-        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl);
+        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl, false);   // batches run unseeded
         StepSums<T, AccT> ss;
         sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
         publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, (int)(u & (NSLOT - 1)));
@@ -1186,12 +1250,19 @@ __global__ void k_batch_window(const MemberD<T> *members, int n, double window)
 }
 
 // --------------------------------------------------------------------------
-// Initial dt: max stable velocity over the initial depth (one thread per
-// cell, run once per run), then the first step's control.
+// Full velocity pass: max stable velocity over the current depth (one
+// thread per cell), then the step control without a time advance. Run once
+// for the first step's dt, and (only_if_needed) after a step whose
+// seed-pruned velocity maximum fell below the seed, so that step's dt comes
+// from every cell.
 
 template <typename T, int K, int MATH>
-__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl)
+__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl, int only_if_needed)
 {
+    // only_if_needed: the full velocity pass after a step whose pruned
+    // maximum fell below its seed (ctl->need_v); otherwise nothing to do
+    if (only_if_needed && ctl->need_v == 0)
+        return;
     const StepK<T> k = rk.k;
     const T *h = ctl->h_cur ? g.h1 : g.h0;
     T vmax = T(0);

@@ -232,7 +232,7 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
         k_volume<float><<<256, 256, 0, s>>>(g, ctl, rk.k.A, vol);
         NA_TRY(cudaGetLastError());
     }
-    NA_TRY(L.init(&g, &rk, tc, ctl, nsm * 4, s));
+    NA_TRY(L.init(&g, &rk, tc, ctl, nsm * 4, s, 0));
     for (int k = 0; k < cfg->max_steps; k++)
         NA_TRY(L.step(&g, &rk, tc, ctl, grid * wpb, grid, s));
     k_unpack<<<512, 256, 0, s>>>(g, ctl, h, hmax, tmax);

@@ -278,6 +278,7 @@ extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *strea
     tc.U = cfg->U > 0 ? cfg->U : 1;
     tc.time_f32 = p == FCAB_PREC_F32_ALL;
     tc.prec_f64 = p == FCAB_PREC_F64;
+    tc.vseed_on = 1;        // sessions launch the full velocity pass after each step
     *out = s;
     return 0;
 }
@@ -562,16 +563,29 @@ static void grid_view(FcabSim *s, GridD<T> &g)
     g.nc = s->cfg.ncols;
 }
 
+// Kernel launches per step: the step, and with seeded dt pruning the
+// guarded full velocity pass (it returns at once unless the step deferred
+// its dt).
+static int launches_per_step(const FcabSim *s) { return s->tc.vseed_on ? 2 : 1; }
+
 static cudaError_t launch_one(FcabSim *s)
 {
+    const int full_grid = 2 * 148 * 4;
+    cudaError_t e;
     if (s->esize == 8) {
         GridD<double> g;
         grid_view(s, g);
-        return s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+        e = s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+        if (e == cudaSuccess && s->tc.vseed_on)
+            e = s->L.init(&g, &s->rkd, s->tc, s->ctl, full_grid, s->stream, 1);
+        return e;
     }
     GridD<float> g;
     grid_view(s, g);
-    return s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+    e = s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+    if (e == cudaSuccess && s->tc.vseed_on)
+        e = s->L.init(&g, &s->rkf, s->tc, s->ctl, full_grid, s->stream, 1);
+    return e;
 }
 
 extern "C" int fcab_sim_reset_time(FcabSim *s, double t, int step, double dt_base, int force_day)
@@ -598,13 +612,13 @@ extern "C" int fcab_sim_reset_time(FcabSim *s, double t, int step, double dt_bas
         grid_view(s, g);
         k_volume<double><<<512, 256, 0, s->stream>>>(g, s->ctl, s->rkd.k.A, vol);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(s->L.init(&g, &s->rkd, s->tc, s->ctl, 2 * 148 * 4, s->stream));
+        CUDA_TRY(s->L.init(&g, &s->rkd, s->tc, s->ctl, 2 * 148 * 4, s->stream, 0));
     } else {
         GridD<float> g;
         grid_view(s, g);
         k_volume<float><<<512, 256, 0, s->stream>>>(g, s->ctl, s->rkf.k.A, vol);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(s->L.init(&g, &s->rkf, s->tc, s->ctl, 2 * 148 * 4, s->stream));
+        CUDA_TRY(s->L.init(&g, &s->rkf, s->tc, s->ctl, 2 * 148 * 4, s->stream, 0));
     }
     s->launches += 2;
     CUDA_TRY(cudaMemcpyAsync(&s->V0, vol, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -647,12 +661,12 @@ extern "C" int fcab_sim_advance(FcabSim *s, int nsteps)
     }
     while (nsteps >= GRAPH_STEPS) {
         CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
-        s->launches += GRAPH_STEPS;
+        s->launches += GRAPH_STEPS * launches_per_step(s);
         nsteps -= GRAPH_STEPS;
     }
     for (; nsteps > 0; nsteps--) {
         CUDA_TRY(launch_one(s));
-        s->launches += 1;
+        s->launches += launches_per_step(s);
     }
     return 0;
 }
@@ -748,6 +762,7 @@ extern "C" int fcab_sim_stats(FcabSim *s, FcabStats *st)
     st->cap_active = cap;
     st->cap_total = s->faces_per_step * (long long)(c->step - s->step0);
     st->dt_min_hits = c->dt_min_hits;
+    st->dt_full_passes = c->full_passes;
     double den = st->V_rain + st->V_in + st->V0;
     if (den < 1e-30)
         den = 1e-30;
@@ -849,6 +864,7 @@ extern "C" int fcab_sim_set_config(FcabSim *s, const FcabConfig *cfg)
     tc.max_steps = cfg->max_steps;
     tc.U = cfg->U > 0 ? cfg->U : 1;
     tc.inflow_ok = inflow_ok;
+    tc.vseed_on = 1;
     s->cpl = cfg->cols_per_lane ? pick_cpl(*cfg) : keep_cpl;
     s->variant_dirty = true;
     return 0;

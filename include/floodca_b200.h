@@ -189,6 +189,7 @@ typedef struct FcabStats {
     double V, V0, V_rain, V_sea, V_bnd, clamp_err, V_in;
     long long cap_active, cap_total, dt_min_hits;
     double E_mass;            /* |V+V_sea+V_bnd-V_rain-V_in-V0-clamp| / (V_rain+V_in+V0) */
+    long long dt_full_passes; /* steps whose dt needed the full velocity pass (seed missed) */
 } FcabStats;
 
 /* Error codes returned by the fcab_* calls (fcab_last_error() has the text). */

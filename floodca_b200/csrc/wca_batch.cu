@@ -45,6 +45,7 @@ struct FcabBatch {
     BatchLaunchers L{};
     MemberD<float> *d_members = nullptr;
     int *d_unit_member = nullptr;
+    int *d_need = nullptr;      // members whose step deferred its dt
     BatchQ *d_q = nullptr;
     int *d_flags = nullptr;
     int *h_flags = nullptr;     // pinned
@@ -111,7 +112,7 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
         d.g.nc = s->cfg.ncols;
         d.rk = s->rkf;
         d.tc = s->tc;
-        d.tc.vseed_on = 0;    // batches prune without a seed (no full pass between steps)
+        d.tc.vseed_on = 1;    // the graph runs the deferred full passes after each step
         d.ctl = s->ctl;
         d.strips = (s->cfg.ncols + ow - 1) / ow;
         d.seg = member_seg_rows && member_seg_rows[i] > 0 ? member_seg_rows[i] : b->seg;
@@ -124,6 +125,8 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
     cudaError_t e = cudaMalloc(&b->d_members, sizeof(MemberD<float>) * n);
     if (e == cudaSuccess)
         e = cudaMalloc(&b->d_unit_member, sizeof(int) * um.size());
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_need, sizeof(int) * n);
     if (e == cudaSuccess)
         e = cudaMalloc(&b->d_q, sizeof(BatchQ));
     if (e == cudaSuccess)
@@ -162,6 +165,7 @@ extern "C" void fcab_batch_destroy(FcabBatch *b)
         cudaGraphExecDestroy(b->graph);
     cudaFree(b->d_members);
     cudaFree(b->d_unit_member);
+    cudaFree(b->d_need);
     cudaFree(b->d_q);
     cudaFree(b->d_flags);
     if (b->h_flags)
@@ -182,9 +186,12 @@ static int batch_graph(FcabBatch *b, int steps)
     if (e != cudaSuccess)
         return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
     cudaError_t le = cudaSuccess;
-    for (int i = 0; i < steps && le == cudaSuccess; i++)
-        le = b->L.step(b->d_members, b->d_unit_member, b->total_units, b->d_q, b->grid,
-                       b->stream);
+    for (int i = 0; i < steps && le == cudaSuccess; i++) {
+        le = b->L.step(b->d_members, b->d_unit_member, b->total_units, b->d_q, b->d_need,
+                       b->grid, b->stream);
+        if (le == cudaSuccess)
+            le = b->L.vfull(b->d_members, b->d_need, b->d_q, 2 * 148 * 4, b->stream);
+    }
     e = cudaStreamEndCapture(b->stream, &g);
     if (le != cudaSuccess || e != cudaSuccess)
         return bfail(FCAB_ERR_CUDA, "fcab_batch: graph capture failed");
@@ -217,7 +224,7 @@ extern "C" int fcab_batch_run(FcabBatch *b, double window_s, int graph_steps, in
         e = cudaGraphLaunch(b->graph, b->stream);
         if (e != cudaSuccess)
             return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
-        b->launches += steps;
+        b->launches += 2 * steps;
         b->replays += 1;
         k_gather_active<<<(b->n + 127) / 128, 128, 0, b->stream>>>(b->d_members, b->n,
                                                                    b->d_flags);

@@ -34,7 +34,10 @@ struct Launchers {
 // Batched-ensemble launchers (FP32 state, FP64 accumulation).
 struct BatchLaunchers {
     cudaError_t (*step)(const void *members, const int *unit_member, int total_units, BatchQ *q,
-                        int grid, cudaStream_t s);
+                        int *need_list, int grid, cudaStream_t s);
+    // full velocity pass of the members whose step deferred its dt
+    cudaError_t (*vfull)(const void *members, const int *need_list, BatchQ *q, int grid,
+                         cudaStream_t s);
     cudaError_t (*window)(const void *members, int n, double window, cudaStream_t s);
     const void *step_fn;
 };
@@ -42,10 +45,19 @@ bool lookup_batch_f32(const VariantKey &k, BatchLaunchers *out);
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LAND>
 cudaError_t launch_batch(const void *members, const int *unit_member, int total_units, BatchQ *q,
-                         int grid, cudaStream_t s)
+                         int *need_list, int grid, cudaStream_t s)
 {
     k_step_batch<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, 128, 0, s>>>(
-        static_cast<const MemberD<T> *>(members), unit_member, total_units, q);
+        static_cast<const MemberD<T> *>(members), unit_member, total_units, q, need_list);
+    return cudaGetLastError();
+}
+
+template <typename T, int K, int MATH>
+cudaError_t launch_batch_vfull(const void *members, const int *need_list, BatchQ *q, int grid,
+                               cudaStream_t s)
+{
+    k_batch_vfull<T, K, MATH><<<grid, 256, 0, s>>>(static_cast<const MemberD<T> *>(members),
+                                                  need_list, q);
     return cudaGetLastError();
 }
 

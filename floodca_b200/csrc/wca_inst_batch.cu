@@ -16,6 +16,7 @@ static bool lookup_batch_math(const VariantKey &k, BatchLaunchers *out)
             out->step_fn = (const void *)&k_step_batch<float, double, KK, CC, MATH, RR, false>; \
         }                                                                                \
         out->window = &launch_window<float>;                                             \
+        out->vfull = &launch_batch_vfull<float, KK, MATH>;                               \
         return true;                                                                     \
     }
     FCAB_BCASE(4, 1, false) FCAB_BCASE(4, 1, true)

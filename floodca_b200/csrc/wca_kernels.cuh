@@ -1179,13 +1179,15 @@ struct MemberD {
 struct BatchQ {
     unsigned int next_unit;
     unsigned int warps_out;
+    unsigned int nneed;         // members whose step deferred its dt (seed missed)
+    unsigned int vfull_out;     // CTAs done with the full velocity passes
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
 __global__ void __launch_bounds__(128, CPL == 2 ? 3 : 1)
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,
-                                                    BatchQ *q)
+                                                    BatchQ *q, int *need_list)
 {
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -1205,7 +1207,7 @@ k_step_batch(const MemberD<T> *members,
         const int local = (int)u - md.unit_off;
         const int strip = local % md.strips, blk = local / md.strips;
         const int r0 = blk * md.seg, r1 = min(g.nr, r0 + md.seg);
-        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl, false);   // batches run unseeded
+        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl);
         StepSums<T, AccT> ss;
         sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
         publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, (int)(u & (NSLOT - 1)));
@@ -1218,6 +1220,8 @@ k_step_batch(const MemberD<T> *members,
                 ctl->launches += 1;
                 const TimeCfg tc = md.tc;
                 finalize<T>(ctl, tc, rk, true);
+                if (ctl->need_v)    // seed missed: the full pass after this launch
+                    need_list[atomicAdd(&q->nneed, 1u)] = m;
             }
         }
         __syncwarp();
@@ -1257,12 +1261,8 @@ __global__ void k_batch_window(const MemberD<T> *members, int n, double window)
 // from every cell.
 
 template <typename T, int K, int MATH>
-__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl, int only_if_needed)
+__device__ void velocity_pass(const GridD<T> &g, const RunK<T> &rk, const TimeCfg &tc, Ctl *ctl)
 {
-    // only_if_needed: the full velocity pass after a step whose pruned
-    // maximum fell below its seed (ctl->need_v); otherwise nothing to do
-    if (only_if_needed && ctl->need_v == 0)
-        return;
     const StepK<T> k = rk.k;
     const T *h = ctl->h_cur ? g.h1 : g.h0;
     T vmax = T(0);
@@ -1321,6 +1321,37 @@ __global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl, int only
         if (prev == gridDim.x - 1) {
             __threadfence();
             finalize<T>(ctl, tc, rk, false);
+        }
+    }
+}
+
+template <typename T, int K, int MATH>
+__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl, int only_if_needed)
+{
+    // only_if_needed: the full velocity pass after a step whose pruned
+    // maximum fell below its seed (ctl->need_v); otherwise nothing to do
+    if (only_if_needed && ctl->need_v == 0)
+        return;
+    velocity_pass<T, K, MATH>(g, rk, tc, ctl);
+}
+
+// The full velocity pass of every batch member whose step deferred its dt
+// (need_list, filled by the step launch before), one member after another
+// over the whole grid; the last CTA out clears the list.
+template <typename T, int K, int MATH>
+__global__ void k_batch_vfull(const MemberD<T> *members, const int *need_list, BatchQ *q)
+{
+    const unsigned nneed = q->nneed;
+    for (unsigned i = 0; i < nneed; i++) {
+        const MemberD<T> &md = members[need_list[i]];
+        velocity_pass<T, K, MATH>(md.g, md.rk, md.tc, md.ctl);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&q->vfull_out, 1u) == gridDim.x - 1u) {
+            q->nneed = 0u;
+            q->vfull_out = 0u;
         }
     }
 }

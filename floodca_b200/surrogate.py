@@ -120,10 +120,9 @@ def train(model, X, Y, Xv=None, Yv=None, epochs: int = 30, batch: int = 32, lr: 
         torch.cuda.synchronize()
         rec = {"epoch": ep + 1, "train_mse": float(tot) / (n // batch * batch * X.shape[1] * X.shape[2]),
                "s": time.perf_counter() - t0}
-        if Xv is not None and (ep + 1) % 5 == 0 or ep + 1 == epochs:
-            if Xv is not None:
-                pv = predict_mean(model, Xv)
-                rec["val_rmse_m"] = float(((pv - from_target(Yv)) ** 2).mean().sqrt())
+        if Xv is not None and ((ep + 1) % 5 == 0 or ep + 1 == epochs):
+            pv = predict_mean(model, Xv)
+            rec["val_rmse_m"] = float(((pv - from_target(Yv)) ** 2).mean().sqrt())
         hist.append(rec)
         if log:
             log(rec)

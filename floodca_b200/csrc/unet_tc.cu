@@ -443,6 +443,229 @@ k_conv_gemm(const __grid_constant__ CUtensorMap tx, const __grid_constant__ CUte
 }
 
 // ---------------------------------------------------------------------------
+// Small-channel convolutions (16- or 32-channel K blocks): one halo'd A tile
+// per super-tile of MT x 128 pixels serves all nine taps. The tile holds the
+// rows p0 - Wp - 1 .. p0 + MT*128 + Wp of the activation matrix in the
+// unswizzled K-major layout: 8-channel planes of 16-byte rows, 8-row groups
+// 128 B apart (SBO) and planes `plane` bytes apart (LBO), i.e. plain linear
+// rows, so tap (ky, kx) of tile t is the same tile read from row
+// t*128 + ky*Wp + kx. Per 128 output pixels this loads (MT*128 + 2*Wp +
+// 2) / MT rows instead of 9 x 128. Weights stay resident (swizzled, as in
+// k_conv_gemm). Same warp roles as k_conv_gemm; TMEM holds two buffers of MT
+// accumulators, TCS columns each.
+
+struct HaloArgs {
+    int P, Hp, Wp;          // padded pixel count, padded height and width
+    int Cin, Cout;
+    int nsup;               // super-tiles of MT x 128 pixels
+    int nkb;                // channel blocks (Cin / CK)
+    int rows_alloc;         // rows per 8-channel plane (multiple of 128)
+    int stages;             // ring stages (one halo tile per channel block)
+    int stage_bytes;        // (CK / 8) x rows_alloc x 16
+    unsigned long long m_hw, m_w;   // ceil(2^48 / (Hp*Wp)), ceil(2^48 / Wp)
+    const float *bias;      // [Cout] or null
+    bf16 *y;                // [P][Cout]
+    int relu;
+};
+
+template <int CK, int BN, int MT>
+struct HaloCfg {
+    static constexpr int NPL = CK / 8;                      // planes per stage
+    static constexpr int B_BYTES = BN * CK * 2;
+    static constexpr int B_AL = (B_BYTES + 1023) / 1024 * 1024;
+    static constexpr uint32_t TCS = BN <= 32 ? 32 : BN <= 64 ? 64 : 128;   // columns per tile
+    static constexpr uint32_t TCOLS = 2 * MT * TCS;         // two buffers of MT tiles
+};
+
+template <int CK, int BN, int MT>
+__global__ void __launch_bounds__(320, 1)
+k_conv_halo(const __grid_constant__ CUtensorMap tx, const __grid_constant__ CUtensorMap tw,
+            HaloArgs a)
+{
+    using Cfg = HaloCfg<CK, BN, MT>;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t *sm = smem_raw + (base - raw);
+    const int S = a.stages;
+    const uint32_t plane = (uint32_t)a.rows_alloc * 16u;
+    const uint32_t bres_off = (uint32_t)(S * a.stage_bytes);
+    const uint32_t bar_off = bres_off + (uint32_t)(9 * a.nkb * Cfg::B_AL);
+    const uint32_t bar0 = base + bar_off;
+    auto full = [&](int s) { return bar0 + 8u * s; };
+    auto empty = [&](int s) { return bar0 + 8u * (S + s); };
+    const uint32_t bfull = bar0 + 16u * S;
+    auto tfull = [&](int b) { return bar0 + 16u * S + 8u + 8u * b; };
+    auto tempty = [&](int b) { return bar0 + 16u * S + 24u + 8u * b; };
+    uint32_t *tslot = (uint32_t *)(sm + bar_off + 16u * S + 40u);
+    float *sbias = (float *)(sm + bar_off + 16u * S + 64u);
+    auto sA = [&](int s) { return base + (uint32_t)(s * a.stage_bytes); };
+    auto sB = [&](int q) { return base + bres_off + (uint32_t)(q * Cfg::B_AL); };
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = threadIdx.x; c < a.Cout; c += blockDim.x)
+        sbias[c] = a.bias ? a.bias[c] : 0.0f;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        mbar_init(bfull, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(tfull(b), 1);
+            mbar_init(tempty(b), 128);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0)
+        tmem_alloc(smem_u32(tslot), Cfg::TCOLS);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const int nkb = a.nkb;
+    const int nbox = a.rows_alloc / 128;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // resident weights: chunk q = tap * nkb + kb holds w[.][tap][kb*CK ..]
+            mbar_expect_tx(bfull, (uint32_t)(9 * nkb * Cfg::B_BYTES));
+            for (int tap = 0; tap < 9; tap++)
+                for (int kb = 0; kb < nkb; kb++)
+                    tma_load_2d(sB(tap * nkb + kb), &tw, bfull, tap * a.Cin + kb * CK, 0);
+            const uint32_t tx_bytes = (uint32_t)(Cfg::NPL * nbox * 128 * 16);
+            int s = 0;
+            uint32_t ph = 0;
+            bool wrapped = false, bad = false;
+            for (int sup = blockIdx.x; sup < a.nsup && !bad; sup += gridDim.x) {
+                const int r0 = sup * MT * 128 - a.Wp - 1;
+                for (int kb = 0; kb < nkb; kb++) {
+                    if (wrapped && !mbar_wait(empty(s), ph ^ 1u)) {
+                        set_err(7);
+                        bad = true;
+                        break;
+                    }
+                    mbar_expect_tx(full(s), tx_bytes);
+                    for (int j = 0; j < Cfg::NPL; j++)
+                        for (int b = 0; b < nbox; b++)
+                            tma_load_2d(sA(s) + (uint32_t)j * plane + (uint32_t)b * 2048u, &tx,
+                                        full(s), kb * CK + 8 * j, r0 + 128 * b);
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                        wrapped = true;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16(128, BN, false, false);
+            bool bad = !mbar_wait(bfull, 0);
+            if (bad)
+                set_err(8);
+            int s = 0, tl = 0;
+            uint32_t ph = 0;
+            for (int sup = blockIdx.x; sup < a.nsup && !bad; sup += gridDim.x, tl++) {
+                const int buf = tl & 1;
+                if (tl >= 2 && !mbar_wait(tempty(buf), (uint32_t)((tl >> 1) - 1) & 1u)) {
+                    set_err(8);
+                    break;
+                }
+                tc_fence_after();
+                for (int kb = 0; kb < nkb; kb++) {
+                    if (!mbar_wait(full(s), ph)) {
+                        set_err(8);
+                        bad = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t st = sA(s);
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int ky = tap >= 6 ? 2 : tap >= 3 ? 1 : 0;
+                        const uint32_t off = (uint32_t)(ky * a.Wp + (tap - 3 * ky)) * 16u;
+                        const uint32_t bb = sB(tap * nkb + kb);
+#pragma unroll
+                        for (int t = 0; t < MT; t++) {
+                            const uint32_t d = tmem + (uint32_t)((buf * MT + t) * Cfg::TCS);
+#pragma unroll
+                            for (int kk = 0; kk < CK / 16; kk++) {
+                                // K = 16: planes 2kk (k 0-7) and 2kk+1 (k 8-15, LBO apart)
+                                const uint32_t aa = st + (uint32_t)(2 * kk) * plane +
+                                                    (uint32_t)(t * 128) * 16u + off;
+                                umma_bf16(d, smem_desc(aa, plane, 128u, 0u),
+                                          kdesc<CK>(bb + 32u * kk), idesc,
+                                          (kb | tap | kk) != 0 ? 1u : 0u);
+                            }
+                        }
+                    }
+                    umma_commit(empty(s));
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                umma_commit(tfull(buf));
+            }
+        }
+    } else {
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int grp = (warp - 2) >> 2;        // epilogue warpgroup = TMEM buffer
+        const int row = q * 32 + lane;
+        const int HW = a.Hp * a.Wp;
+        int k = 0;
+        for (int sup = blockIdx.x + grp * gridDim.x; sup < a.nsup; sup += 2 * gridDim.x, k++) {
+            if (!mbar_wait(tfull(grp), (uint32_t)k & 1u)) {
+                set_err(9);
+                break;
+            }
+            __syncwarp();
+            tc_fence_after();
+#pragma unroll 1
+            for (int t = 0; t < MT; t++) {
+                const int p = (sup * MT + t) * 128 + row;
+                bool store = p < a.P;
+                if (store) {
+                    const int qq = p - HW * div_m(p, a.m_hw);
+                    const int yy = div_m(qq, a.m_w);
+                    const int xx = qq - yy * a.Wp;
+                    store = yy >= 1 && yy <= a.Hp - 2 && xx >= 1 && xx <= a.Wp - 2;
+                }
+                const uint32_t t0 = tmem + (uint32_t)((grp * MT + t) * Cfg::TCS) +
+                                    ((uint32_t)(q * 32) << 16);
+#pragma unroll 1
+                for (int c = 0; c < BN; c += 32) {
+                    float v[32];
+                    tmem_ld32(t0 + (uint32_t)c, v);
+                    if (store) {
+                        __align__(16) bf16 o[32];
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            float x = v[j] + sbias[c + j];
+                            if (a.relu)
+                                x = fmaxf(x, 0.0f);
+                            o[j] = __float2bfloat16_rn(x);
+                        }
+                        uint4 *dst = (uint4 *)(a.y + (size_t)p * a.Cout + c);
+                        const uint4 *src = (const uint4 *)o;
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            dst[j] = src[j];
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(tempty(grp));
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        tmem_dealloc(tmem, Cfg::TCOLS);
+}
+
+// ---------------------------------------------------------------------------
 // Weight gradient: dW[co][tap][ci] += sum_p dY[p][co] * X[p + shift(tap)][ci]
 // as M = 128 output channels x N = 64*NB input channels x K = pixels, both
 // operands MN-major (channels contiguous): each is loaded as boxes of 64
@@ -1062,6 +1285,82 @@ cudaError_t gemm_bn(const CUtensorMap &tx, const CUtensorMap &tw, const GemmArgs
     }
 }
 
+template <int CK, int BN, int MT>
+cudaError_t launch_halo(const CUtensorMap &txh, const CUtensorMap &tw, const HaloArgs &a, int smem,
+                        cudaStream_t st)
+{
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr_set[dev & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv_halo<CK, BN, MT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_MAX);
+        if (e != cudaSuccess)
+            return e;
+        attr_set[dev & 63] = true;
+    }
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = a.nsup < nsm ? a.nsup : nsm;
+    k_conv_halo<CK, BN, MT><<<grid, 320, smem, st>>>(txh, tw, a);
+    return cudaGetLastError();
+}
+
+// The halo path for 16/32-channel K blocks and one output tile of at most
+// 128 channels, when its tiles fit in shared memory. Returns
+// cudaErrorNotSupported when the shape does not qualify (the caller then
+// uses k_conv_gemm).
+template <int CK>
+cudaError_t try_halo(const void *x, const CUtensorMap &tw, int N, int H, int W, int Cin, int Cout,
+                     const float *bias, int relu, void *y, cudaStream_t st)
+{
+    if (Cout > 128)
+        return cudaErrorNotSupported;
+    const int MT = Cout <= 64 ? 4 : 2;
+    const long long P = (long long)N * (H + 2) * (W + 2);
+    const int Wp = W + 2;
+    const int rows = MT * 128 + 2 * Wp + 2;
+    const int rows_alloc = (rows + 127) / 128 * 128;
+    if (rows_alloc * 16 >= (1 << 18))          // LBO field limit
+        return cudaErrorNotSupported;
+    const int nkb = Cin / CK;
+    const int bn_al = (Cout * CK * 2 + 1023) / 1024 * 1024;
+    const int bres = 9 * nkb * bn_al;
+    const int stage = (CK / 8) * rows_alloc * 16;
+    const int fixed = 1024 + bres + 64 + 4 * Cout;
+    int stages = (SMEM_MAX - fixed) / (stage + 16);
+    stages = stages > 4 ? 4 : stages;
+    if (stages < 2)
+        return cudaErrorNotSupported;
+    CUtensorMap txh;
+    if (!make_map(&txh, x, P, Cin, 8, 128, CU_TENSOR_MAP_SWIZZLE_NONE))
+        return cudaErrorInvalidValue;
+    HaloArgs a;
+    a.P = (int)P;
+    a.Hp = H + 2;
+    a.Wp = Wp;
+    a.Cin = Cin;
+    a.Cout = Cout;
+    a.nsup = (int)((P + MT * 128 - 1) / (MT * 128));
+    a.nkb = nkb;
+    a.rows_alloc = rows_alloc;
+    a.stages = stages;
+    a.stage_bytes = stage;
+    a.m_hw = ((1ull << 48) + (unsigned long long)(a.Hp * a.Wp) - 1) / (unsigned long long)(a.Hp * a.Wp);
+    a.m_w = ((1ull << 48) + (unsigned long long)a.Wp - 1) / (unsigned long long)a.Wp;
+    a.bias = bias;
+    a.y = (bf16 *)y;
+    a.relu = relu;
+    const int smem = fixed + stages * (stage + 16);
+    switch (Cout) {
+    case 32: return launch_halo<CK, 32, 4>(txh, tw, a, smem, st);
+    case 64: return launch_halo<CK, 64, 4>(txh, tw, a, smem, st);
+    case 96: return launch_halo<CK, 96, 2>(txh, tw, a, smem, st);
+    case 128: return launch_halo<CK, 128, 2>(txh, tw, a, smem, st);
+    default: return cudaErrorNotSupported;
+    }
+}
+
 // y[P][Cout] = conv3x3(x[P][Cin], w[Cout][9][Cin]) (+ bias, ReLU).
 int conv_gemm(const void *x, int N, int H, int W, int Cin, const void *w, int Cout,
               const float *bias, int relu, void *y, cudaStream_t st)
@@ -1083,6 +1382,14 @@ int conv_gemm(const void *x, int N, int H, int W, int Cin, const void *w, int Co
     CUtensorMap tx, tw;
     if (!make_map(&tx, x, P, Cin, CK, 128, sw) || !make_map(&tw, w, Cout, 9 * Cin, CK, bn, sw))
         return fail(FCAB_ERR_CUDA, "conv: tensor map encoding failed");
+    if (CK <= 32 && bn == Cout) {
+        const cudaError_t he = CK == 32 ? try_halo<32>(x, tw, N, H, W, Cin, Cout, bias, relu, y, st)
+                                        : try_halo<16>(x, tw, N, H, W, Cin, Cout, bias, relu, y, st);
+        if (he == cudaSuccess)
+            return 0;
+        if (he != cudaErrorNotSupported)
+            return fail(FCAB_ERR_CUDA, cudaGetErrorString(he));
+    }
     GemmArgs a;
     a.P = (int)P;
     a.Hp = H + 2;

@@ -75,6 +75,9 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
         if (s->tc.n_force_days > 0 || s->tc.progress_every > 0)
             return bfail(FCAB_ERR_ARG, "fcab_batch_create: members with forcing days or "
                                        "progress pauses run as single sessions");
+        if (s->slab)
+            return bfail(FCAB_ERR_ARG, "fcab_batch_create: a slab of a row-split domain "
+                                       "steps through fcab_sim_slab_*");
     }
     FcabBatch *b = new FcabBatch();
     b->members.assign(members, members + n);
@@ -110,6 +113,8 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
         d.g.pitch = s->pitch;
         d.g.nr = s->cfg.nrows;
         d.g.nc = s->cfg.ncols;
+        d.g.r_lo = 0;
+        d.g.r_hi = s->cfg.nrows;
         d.rk = s->rkf;
         d.tc = s->tc;
         d.tc.vseed_on = 1;    // the graph runs the deferred full passes after each step

@@ -57,6 +57,7 @@ struct GridD {
     T *h0, *h1, *hmax, *tmax;
     long long pitch;
     int nr, nc;
+    int r_lo, r_hi;             // rows of real cells: [0, nr), or with a slab's halo rows
 };
 
 // Uniform run constants.
@@ -80,7 +81,9 @@ struct Ctl {
     // prepared for the next step by the previous step's last CTA
     double t, dt, F, tmax_val, inflow_dh, t_next, dt_base;
     int step, hit, active, h_cur, want_v, done, pause, force_day;
-    int err, n_force_days, pad0, pad1;
+    int err, n_force_days;
+    int fin_pending;            // slab runs: 1 after a step, 2 after the first velocity pass
+    int pad1;
     long long dt_min_hits;
     unsigned long long vmax_bits;
     unsigned int ctas_done;
@@ -107,7 +110,8 @@ struct TimeCfg {
     int hyeto, max_steps, U, time_f32;
     int n_force_days, progress_every, inflow_ok, prec_f64;
     int vseed_on;               // seed the dt pruning (the launcher adds the full pass)
-    int pad_tc;
+    int split;                  // slab of a row-split domain: the step control waits for
+                                // the velocity maximum reduced over all slabs
 };
 
 // --------------------------------------------------------------------------
@@ -808,7 +812,7 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
             // open-edge terms exist only on open edge rows or edge lanes
             const bool open2 = edge_lane || (rk.open && ((r == 0 && rk.edge_n) ||
                                                          (r == nr - 1 && rk.edge_s)));
-            const bool row2_in = r >= 0 && r < nr;
+            const bool row2_in = r >= g.r_lo && r < g.r_hi;
             // stage-E threshold: the warp's running velocity maximum
             T thr = want_v ? warp_max_nonneg(vmax) : T(0);
             thr = thr > vseed ? thr : vseed;
@@ -1156,7 +1160,12 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(), step_min_blocks<K, 
             __threadfence();
             ctl->h_cur ^= 1;
             ctl->launches += 1;
-            finalize<T>(ctl, tc, rk, true);
+            if (tc.split) {
+                ctl->fin_pending = 1;
+                ctl->ctas_done = 0u;
+            } else {
+                finalize<T>(ctl, tc, rk, true);
+            }
         }
     }
 }
@@ -1323,7 +1332,12 @@ __device__ void velocity_pass(const GridD<T> &g, const RunK<T> &rk, const TimeCf
         const unsigned prev = atomicAdd(&ctl->ctas_done, 1u);
         if (prev == gridDim.x - 1) {
             __threadfence();
-            finalize<T>(ctl, tc, rk, false);
+            if (tc.split) {
+                ctl->fin_pending = 2;
+                ctl->ctas_done = 0u;
+            } else {
+                finalize<T>(ctl, tc, rk, false);
+            }
         }
     }
 }
@@ -1376,6 +1390,43 @@ __global__ void k_volume(GridD<T> g, const Ctl *ctl, T A, double *out)
     v = warp_sum(v);
     if ((threadIdx.x & 31) == 0 && v != 0.0)
         atomicAdd(out, v);
+}
+
+// --------------------------------------------------------------------------
+// Slabs of a row-split domain. Each slab holds its own rows plus up to three
+// halo rows of each neighbour in its padding rows; the step kernel and the
+// velocity pass leave the step control pending (fin_pending) with the
+// slab's own velocity maximum in vmax_bits. Once vmax_bits holds the maximum
+// over all slabs, every slab prepares the same next step here, as one
+// domain would (FloodCA src/common/model.c:111-156 reduces dt the same way
+// through comm->min_real).
+
+template <typename T>
+__global__ void k_slab_finalize(RunK<T> rk, TimeCfg tc, Ctl *ctl)
+{
+    const int p = ctl->fin_pending;
+    if (p == 0)
+        return;
+    ctl->fin_pending = 0;
+    finalize<T>(ctl, tc, rk, p == 1);
+}
+
+// Copies rows [row0, row0 + nrows) of the current depth to a dense
+// nrows x nc buffer (to_buf) or back; rows may lie in the halo.
+template <typename T>
+__global__ void k_rows_copy(const Ctl *ctl, T *h0, T *h1, long long pitch, int row0, int nrows,
+                            int nc, T *buf, int to_buf)
+{
+    T *h = ctl->h_cur ? h1 : h0;
+    const long long N = (long long)nrows * nc;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long a = (long long)(row0 + i / nc + PADR) * pitch + i % nc + PADC;
+        if (to_buf)
+            buf[i] = h[a];
+        else
+            h[a] = buf[i];
+    }
 }
 
 }  // namespace fcab

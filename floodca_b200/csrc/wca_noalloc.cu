@@ -174,6 +174,8 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     g.pitch = pitch;
     g.nr = cfg->nrows;
     g.nc = cfg->ncols;
+    g.r_lo = 0;
+    g.r_hi = cfg->nrows;
 
     // The array keeps the previous call's contents: clear everything that
     // must start at zero (control block, padding, accumulators).

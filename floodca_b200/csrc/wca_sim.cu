@@ -7,6 +7,7 @@
 // end the run or to serve a pause (forcing-day reload, progress line).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -48,12 +49,13 @@ int fail(int code, const char *fmt, ...)
 
 constexpr int GRAPH_STEPS = 32;
 
-__global__ void k_fill_interior(void *p, long long pitch, int nr, int nc, double v, int esize)
+__global__ void k_fill_interior(void *p, long long pitch, int r_lo, int nr, int nc, double v,
+                                int esize)
 {
     const long long N = (long long)nr * nc;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long a = (i / nc + PADR) * pitch + i % nc + PADC;
+        const long long a = (r_lo + i / nc + PADR) * pitch + i % nc + PADC;
         if (esize == 8)
             static_cast<double *>(p)[a] = v;
         else
@@ -78,13 +80,13 @@ __global__ void k_fill_all(void *p, long long n, double v, int esize)
 // so a uniform field can be detected exactly.
 template <typename T>
 __global__ void k_make_cr(const T *C, const T *R, const uint8_t *m, T *cr, long long pitch,
-                          int nr, int nc, unsigned long long *mm)
+                          int r_lo, int nr, int nc, unsigned long long *mm)
 {
     unsigned long long lo = ~0ull, hi = 0ull;
     const long long N = (long long)nr * nc;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(i / nc), c = (int)(i % nc);
+        const int r = r_lo + (int)(i / nc), c = (int)(i % nc);
         const long long a = (long long)(r + PADR) * pitch + c + PADC;
         const T v = C[a] * R[a];
         cr[a] = v;
@@ -155,8 +157,10 @@ extern "C" void fcab_config_defaults(FcabConfig *c, int nrows, int ncols)
 
 static double as_real(double v, int prec) { return prec == FCAB_PREC_F64 ? v : (double)(float)v; }
 
+// hn, hs: halo rows above and below a slab's own rows; the inflow cell then
+// indexes the uploaded (hn + nrows + hs) x ncols array.
 template <typename T>
-static void fill_runk(RunK<T> &rk, const FcabConfig &c)
+static void fill_runk(RunK<T> &rk, const FcabConfig &c, int hn = 0, int hs = 0)
 {
     memset(&rk, 0, sizeof(rk));
     StepK<T> &k = rk.k;
@@ -185,8 +189,8 @@ static void fill_runk(RunK<T> &rk, const FcabConfig &c)
     rk.edge_w = c.edge_w;
     rk.edge_e = c.edge_e;
     rk.inflow_r = rk.inflow_c = -1;
-    if (c.inflow_cell >= 0 && c.inflow_cell < (long long)c.nrows * c.ncols) {
-        rk.inflow_r = (int)(c.inflow_cell / c.ncols);
+    if (c.inflow_cell >= 0 && c.inflow_cell < (long long)(c.nrows + hn + hs) * c.ncols) {
+        rk.inflow_r = (int)(c.inflow_cell / c.ncols) - hn;
         rk.inflow_c = (int)(c.inflow_cell % c.ncols);
     }
 }
@@ -304,13 +308,14 @@ extern "C" void fcab_sim_destroy(FcabSim *s)
 }
 
 // Copies a row-major nrows x ncols array (host or device) into the interior of
-// a padded field.
+// a padded field; a slab's arrays carry its halo rows too.
 static cudaError_t put_field(FcabSim *s, void *dst, const void *src, size_t esz,
                              cudaMemcpyKind kind)
 {
-    char *d = (char *)dst + ((size_t)PADR * s->pitch + PADC) * esz;
+    char *d = (char *)dst + ((size_t)(PADR - s->hn) * s->pitch + PADC) * esz;
     return cudaMemcpy2DAsync(d, (size_t)s->pitch * esz, src, (size_t)s->cfg.ncols * esz,
-                             (size_t)s->cfg.ncols * esz, (size_t)s->cfg.nrows, kind, s->stream);
+                             (size_t)s->cfg.ncols * esz, (size_t)(s->cfg.nrows + s->hn + s->hs),
+                             kind, s->stream);
 }
 
 static cudaError_t get_field(FcabSim *s, void *dst, const void *src, size_t esz)
@@ -325,7 +330,8 @@ static int fill_interior(FcabSim *s, void *dst, double v)
 {
     // Padding stays zero; the nrows x ncols interior gets v.
     CUDA_TRY(cudaMemsetAsync(dst, 0, s->nelem * s->esize, s->stream));
-    k_fill_interior<<<1024, 256, 0, s->stream>>>(dst, s->pitch, s->cfg.nrows, s->cfg.ncols, v,
+    k_fill_interior<<<1024, 256, 0, s->stream>>>(dst, s->pitch, -s->hn,
+                                                 s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, v,
                                                  (int)s->esize);
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -344,11 +350,11 @@ static int rebuild_rain(FcabSim *s)
     if (s->esize == 8)
         k_make_cr<double><<<nb, 256, 0, s->stream>>>(
             (const double *)s->tmpC, (const double *)s->tmpR, s->m, (double *)s->cr, s->pitch,
-            s->cfg.nrows, s->cfg.ncols, (unsigned long long *)s->scratch);
+            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch);
     else
         k_make_cr<float><<<nb, 256, 0, s->stream>>>(
             (const float *)s->tmpC, (const float *)s->tmpR, s->m, (float *)s->cr, s->pitch,
-            s->cfg.nrows, s->cfg.ncols, (unsigned long long *)s->scratch);
+            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch);
     CUDA_TRY(cudaGetLastError());
     unsigned long long mm[2];
     CUDA_TRY(cudaMemcpyAsync(mm, s->scratch, sizeof(mm), cudaMemcpyDeviceToHost, s->stream));
@@ -425,13 +431,15 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
     // has SEA / inflow cell LAND
     std::vector<uint8_t> probe;
     const long long N = (long long)c.nrows * c.ncols;
-    const uint8_t *mh = mask;
+    const long long Nup = (long long)(c.nrows + s->hn + s->hs) * c.ncols;   // with halo rows
+    const uint8_t *mup = mask;
     if (kind != cudaMemcpyHostToDevice) {
-        probe.resize((size_t)N);
-        CUDA_TRY(cudaMemcpy(probe.data(), mask, (size_t)N, cudaMemcpyDeviceToHost));
-        mh = probe.data();
+        probe.resize((size_t)Nup);
+        CUDA_TRY(cudaMemcpy(probe.data(), mask, (size_t)Nup, cudaMemcpyDeviceToHost));
+        mup = probe.data();
     }
-    const int has_sea = memchr(mh, M_SEA, (size_t)N) != nullptr;
+    const uint8_t *mh = mup + (long long)s->hn * c.ncols;              // own rows
+    const int has_sea = memchr(mup, M_SEA, (size_t)Nup) != nullptr;
     // LAND cells per row; open faces only on the open edges' rows/columns
     s->land_cells = 0;
     s->open_faces = 0;
@@ -449,7 +457,12 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
     }
     // all-LAND grids use the mask-free kernel: padding elevation PAD_Z makes
     // every face to the padding carry zero discharge (needs tau_h > 0)
-    const bool all_land = c.tau_h > 0.0 && s->land_cells == N;
+    long long land_up = s->land_cells;       // with a slab's halo rows
+    for (long long k = 0; k < (long long)s->hn * c.ncols; k++)
+        land_up += mup[k] == M_LAND;
+    for (long long k = N + (long long)s->hn * c.ncols; k < Nup; k++)
+        land_up += mup[k] == M_LAND;
+    const bool all_land = c.tau_h > 0.0 && s->land_cells == N && land_up == Nup;
     s->landonly = all_land;
     if (all_land) {
         k_fill_all<<<1024, 256, 0, s->stream>>>(s->z, (long long)s->nelem, PAD_Z, (int)es);
@@ -457,11 +470,13 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
         CUDA_TRY(put_field(s, s->z, z, es, kind));
     }
     int inflow_ok = 0;
-    if (c.inflow_cell >= 0 && c.inflow_cell < N)
-        inflow_ok = mh[c.inflow_cell] == M_LAND;
+    if (c.inflow_cell >= 0 && c.inflow_cell < Nup)
+        inflow_ok = mup[c.inflow_cell] == M_LAND;
     const long long nr = c.nrows, nc = c.ncols;
-    s->faces_per_step = nr * (nc - 1) + (nr - 1) * nc +
-                        (c.K == 8 ? 2 * (nr - 1) * (nc - 1) : 0) + s->open_faces;
+    // a slab also owns the faces between its last row and the south halo
+    const long long ny = nr - 1 + (s->hs > 0 ? 1 : 0);
+    s->faces_per_step = nr * (nc - 1) + ny * nc + (c.K == 8 ? 2 * ny * (nc - 1) : 0) +
+                        s->open_faces;
     if (s->esize == 8) {
         s->rkd.has_sea = has_sea;
     } else {
@@ -561,6 +576,8 @@ static void grid_view(FcabSim *s, GridD<T> &g)
     g.pitch = s->pitch;
     g.nr = s->cfg.nrows;
     g.nc = s->cfg.ncols;
+    g.r_lo = -s->hn;
+    g.r_hi = s->cfg.nrows + s->hs;
 }
 
 // Kernel launches per step: the step, and with seeded dt pruning the
@@ -651,6 +668,8 @@ extern "C" int fcab_sim_advance(FcabSim *s, int nsteps)
 {
     if (!s->inited)
         return fail(FCAB_ERR_STATE, "advance before upload");
+    if (s->slab)
+        return fail(FCAB_ERR_STATE, "a slab steps through fcab_sim_slab_step");
     int rc = resolve_variant(s);
     if (rc)
         return rc;
@@ -842,11 +861,11 @@ extern "C" int fcab_sim_set_config(FcabSim *s, const FcabConfig *cfg)
     const int inflow_ok = s->tc.inflow_ok;
     s->cfg = *cfg;
     if (s->esize == 8) {
-        fill_runk<double>(s->rkd, *cfg);
+        fill_runk<double>(s->rkd, *cfg, s->hn, s->hs);
         s->rkd.has_sea = has_sea;
         s->rkd.cr_uniform = cru;
     } else {
-        fill_runk<float>(s->rkf, *cfg);
+        fill_runk<float>(s->rkf, *cfg, s->hn, s->hs);
         s->rkf.has_sea = has_sea;
         s->rkf.cr_uniform = (float)cru;
     }
@@ -976,6 +995,135 @@ extern "C" int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, u
 }
 
 extern "C" void *fcab_sim_stream(FcabSim *s) { return (void *)s->stream; }
+
+// ---------------------------------------------------------------------------
+// Slabs of a row-split domain.
+
+static_assert(FCAB_SLAB_HALO < PADR, "halo rows live in the padding rows");
+
+extern "C" int fcab_sim_set_slab(FcabSim *s, int halo_n, int halo_s)
+{
+    if (s->uploaded)
+        return fail(FCAB_ERR_STATE, "set_slab after upload");
+    if (halo_n < 0 || halo_n > FCAB_SLAB_HALO || halo_s < 0 || halo_s > FCAB_SLAB_HALO)
+        return fail(FCAB_ERR_ARG, "halo rows %d / %d outside 0..%d", halo_n, halo_s,
+                    FCAB_SLAB_HALO);
+    s->slab = true;
+    s->hn = halo_n;
+    s->hs = halo_s;
+    if (s->esize == 8)
+        fill_runk<double>(s->rkd, s->cfg, s->hn, s->hs);
+    else
+        fill_runk<float>(s->rkf, s->cfg, s->hn, s->hs);
+    // the seed and the deferral decision come from the reduced maximum, so
+    // every slab defers alike; the driver then runs fcab_sim_slab_vfull
+    s->tc.split = 1;
+    s->variant_dirty = true;
+    return 0;
+}
+
+extern "C" int fcab_sim_slab_step(FcabSim *s)
+{
+    if (!s->slab)
+        return fail(FCAB_ERR_STATE, "slab_step on a session that is not a slab");
+    if (!s->inited)
+        return fail(FCAB_ERR_STATE, "slab_step before upload");
+    int rc = resolve_variant(s);
+    if (rc)
+        return rc;
+    if (s->esize == 8) {
+        GridD<double> g;
+        grid_view(s, g);
+        CUDA_TRY(s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream));
+    } else {
+        GridD<float> g;
+        grid_view(s, g);
+        CUDA_TRY(s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream));
+    }
+    s->launches += 1;
+    return 0;
+}
+
+extern "C" int fcab_sim_slab_vfull(FcabSim *s)
+{
+    if (!s->slab)
+        return fail(FCAB_ERR_STATE, "slab_vfull on a session that is not a slab");
+    if (!s->inited)
+        return fail(FCAB_ERR_STATE, "slab_vfull before upload");
+    int rc = resolve_variant(s);
+    if (rc)
+        return rc;
+    const int full_grid = 2 * 148 * 4;
+    if (s->esize == 8) {
+        GridD<double> g;
+        grid_view(s, g);
+        CUDA_TRY(s->L.init(&g, &s->rkd, s->tc, s->ctl, full_grid, s->stream, 1));
+    } else {
+        GridD<float> g;
+        grid_view(s, g);
+        CUDA_TRY(s->L.init(&g, &s->rkf, s->tc, s->ctl, full_grid, s->stream, 1));
+    }
+    s->launches += 1;
+    return 0;
+}
+
+extern "C" int fcab_sim_slab_vmax(FcabSim *s, unsigned long long **vmax)
+{
+    if (!s->slab)
+        return fail(FCAB_ERR_STATE, "slab_vmax on a session that is not a slab");
+    *vmax = &s->ctl->vmax_bits;
+    return 0;
+}
+
+extern "C" int fcab_sim_slab_finalize(FcabSim *s)
+{
+    if (!s->slab)
+        return fail(FCAB_ERR_STATE, "slab_finalize on a session that is not a slab");
+    if (s->esize == 8)
+        k_slab_finalize<double><<<1, 1, 0, s->stream>>>(s->rkd, s->tc, s->ctl);
+    else
+        k_slab_finalize<float><<<1, 1, 0, s->stream>>>(s->rkf, s->tc, s->ctl);
+    CUDA_TRY(cudaGetLastError());
+    s->launches += 1;
+    return 0;
+}
+
+static int rows_copy(FcabSim *s, int row0, int nrows, void *buf, int to_buf)
+{
+    if (!s->uploaded)
+        return fail(FCAB_ERR_STATE, "rows copy before upload");
+    if (nrows < 0 || row0 < -s->hn || (long long)row0 + nrows > (long long)s->cfg.nrows + s->hs)
+        return fail(FCAB_ERR_ARG, "rows [%d, %d) outside %d..%d", row0, row0 + nrows, -s->hn,
+                    s->cfg.nrows + s->hs);
+    if (nrows == 0)
+        return 0;
+    if (!buf)
+        return fail(FCAB_ERR_ARG, "rows copy without a buffer");
+    const long long N = (long long)nrows * s->cfg.ncols;
+    const int blocks = (int)std::min<long long>((N + 255) / 256, 1024);
+    if (s->esize == 8)
+        k_rows_copy<double><<<blocks, 256, 0, s->stream>>>(s->ctl, (double *)s->h0,
+                                                           (double *)s->h1, s->pitch, row0,
+                                                           nrows, s->cfg.ncols, (double *)buf,
+                                                           to_buf);
+    else
+        k_rows_copy<float><<<blocks, 256, 0, s->stream>>>(s->ctl, (float *)s->h0,
+                                                          (float *)s->h1, s->pitch, row0, nrows,
+                                                          s->cfg.ncols, (float *)buf, to_buf);
+    CUDA_TRY(cudaGetLastError());
+    s->launches += 1;
+    return 0;
+}
+
+extern "C" int fcab_sim_rows_get(FcabSim *s, int row0, int nrows, void *dst)
+{
+    return rows_copy(s, row0, nrows, dst, 1);
+}
+
+extern "C" int fcab_sim_rows_put(FcabSim *s, int row0, int nrows, const void *src)
+{
+    return rows_copy(s, row0, nrows, const_cast<void *>(src), 0);
+}
 
 // Evaluates one device math helper over n inputs, for tests: which = 0
 // RN(cbrt(x*x)) (exact mode), 1 min(x, RN(sqrt(g*y))) (exact mode), 2 the

@@ -37,6 +37,10 @@ struct FcabSim {
     int step0 = 0;
     double V0 = 0.0;
     long long land_cells = 0, open_faces = 0, faces_per_step = 0;
+    // slab of a row-split domain: halo rows above (hn) and below (hs) the
+    // session's own rows, carried by every uploaded array
+    bool slab = false;
+    int hn = 0, hs = 0;
 };
 
 namespace fcab {

@@ -62,6 +62,13 @@ def core() -> C.CDLL:
                                              C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
         "fcab_sim_launches": (C.c_longlong, [_P]),
         "fcab_sim_stream": (_P, [_P]),
+        "fcab_sim_set_slab": (C.c_int, [_P, _I, _I]),
+        "fcab_sim_slab_step": (C.c_int, [_P]),
+        "fcab_sim_slab_vfull": (C.c_int, [_P]),
+        "fcab_sim_slab_vmax": (C.c_int, [_P, C.POINTER(_P)]),
+        "fcab_sim_slab_finalize": (C.c_int, [_P]),
+        "fcab_sim_rows_get": (C.c_int, [_P, _I, _I, _P]),
+        "fcab_sim_rows_put": (C.c_int, [_P, _I, _I, _P]),
         "fcab_sim_destroy": (None, [_P]),
         "fcab_math_probe": (C.c_int, [C.c_int, _P, _P, _P, C.c_longlong, C.c_float]),
         "fcab_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int,

@@ -282,6 +282,46 @@ FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uin
 /* The session's cudaStream_t. */
 FCAB_API void *fcab_sim_stream(FcabSim *s);
 
+/* ---- Slabs of a row-split domain (the reference's distributed run:
+ * owned rows [r0, r1) of FcaGrid, src/common/fca_types.h:103-104, with
+ * comm->halo and comm->min_real, src/common/model.c:143-144,359-360,
+ * 507-508). A slab session holds its own rows (FcabConfig.nrows) plus up
+ * to FCAB_SLAB_HALO rows of each neighbour; its step leaves the dt decision
+ * pending until the velocity maximum has been max-reduced over all slabs. */
+#define FCAB_SLAB_HALO 3
+
+/* Before the upload: makes the session a slab with halo_n / halo_s halo
+ * rows above / below (0..FCAB_SLAB_HALO; 0 on a domain edge). Every array
+ * uploaded afterwards (fcab_sim_upload*, fcab_sim_set_rain,
+ * fcab_sim_upload_state) carries halo_n + nrows + halo_s rows, and
+ * FcabConfig.inflow_cell indexes such an array. Internal edges must be
+ * closed in FcabConfig.edge_*. Slabs step only through fcab_sim_slab_*. */
+FCAB_API int fcab_sim_set_slab(FcabSim *s, int halo_n, int halo_s);
+
+/* One step on the slab's own rows; the next step's dt stays pending. */
+FCAB_API int fcab_sim_slab_step(FcabSim *s);
+
+/* The full velocity pass over the slab's own rows, when the last
+ * fcab_sim_slab_finalize deferred dt (the reduced maximum of the seed-pruned
+ * step fell below the seed; every slab defers alike); otherwise it returns at
+ * once. The next step's dt is then pending again. */
+FCAB_API int fcab_sim_slab_vfull(FcabSim *s);
+
+/* Device address of the pending velocity maximum (an unsigned 64-bit
+ * integer holding the bits of a non-negative float or double, so that an
+ * integer max over slabs is the maximum velocity). */
+FCAB_API int fcab_sim_slab_vmax(FcabSim *s, unsigned long long **vmax);
+
+/* Prepares the next step from the (reduced) pending maximum; does nothing
+ * when no decision is pending. */
+FCAB_API int fcab_sim_slab_finalize(FcabSim *s);
+
+/* Copies rows [row0, row0 + nrows) of the current depth (rows -halo_n ..
+ * nrows + halo_s - 1) to a dense nrows x ncols device buffer, or back, in
+ * the session's element type, on the session's stream. */
+FCAB_API int fcab_sim_rows_get(FcabSim *s, int row0, int nrows, void *dst);
+FCAB_API int fcab_sim_rows_put(FcabSim *s, int row0, int nrows, const void *src);
+
 /* ---- Batched ensembles (no reference counterpart; the reference runs
  * members one at a time, src/hybrid/main_ens_mpi_cuda.c:69-120). ---- */
 typedef struct FcabBatch FcabBatch;

@@ -33,7 +33,7 @@ NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPI
            "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC)]
 
 CORE_SRCS = ["wca_inst_f32.cu", "wca_inst_f32all.cu", "wca_inst_f64.cu", "wca_inst_batch.cu",
-             "wca_sim.cu", "wca_noalloc.cu", "wca_batch.cu", "unet_tc.cu"]
+             "wca_sim.cu", "host_copy.cu", "mem_cache.cu", "wca_noalloc.cu", "wca_batch.cu", "unet_tc.cu"]
 
 
 def _deps_newer(obj: Path, srcs: list[Path]) -> bool:

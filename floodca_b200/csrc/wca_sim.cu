@@ -249,16 +249,16 @@ extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *strea
     const size_t fb = s->nelem * s->esize;
     void **fields[] = {&s->z, &s->n, &s->h0, &s->h1, &s->hmax, &s->tmax};
     for (void **f : fields) {
-        e = cudaMalloc(f, fb);
+        e = fcab::cached_malloc(f, fb);
         if (e != cudaSuccess) {
             fcab_sim_destroy(s);
             return fail(FCAB_ERR_CUDA, "cudaMalloc(%zu): %s", fb, cudaGetErrorString(e));
         }
     }
-    if ((e = cudaMalloc(&s->m, s->nelem)) != cudaSuccess ||
-        (e = cudaMalloc(&s->ctl, sizeof(Ctl))) != cudaSuccess ||
-        (e = cudaMalloc(&s->scratch, 64)) != cudaSuccess ||
-        (e = cudaMallocHost(&s->ctl_host, sizeof(Ctl))) != cudaSuccess) {
+    if ((e = fcab::cached_malloc((void **)&s->m, s->nelem)) != cudaSuccess ||
+        (e = fcab::cached_malloc((void **)&s->ctl, sizeof(Ctl))) != cudaSuccess ||
+        (e = fcab::cached_malloc(&s->scratch, 64)) != cudaSuccess ||
+        (e = fcab::cached_malloc_host(&s->ctl_host, sizeof(Ctl))) != cudaSuccess) {
         fcab_sim_destroy(s);
         return fail(FCAB_ERR_CUDA, "allocation: %s", cudaGetErrorString(e));
     }
@@ -299,9 +299,9 @@ extern "C" void fcab_sim_destroy(FcabSim *s)
                     s->scratch, s->tmpC, s->tmpR};
     for (void *q : ptrs)
         if (q)
-            cudaFree(q);
+            fcab::cached_free(q);
     if (s->ctl_host)
-        cudaFreeHost(s->ctl_host);
+        fcab::cached_free(s->ctl_host);
     if (s->own_stream && s->stream)
         cudaStreamDestroy(s->stream);
     delete s;
@@ -313,17 +313,19 @@ static cudaError_t put_field(FcabSim *s, void *dst, const void *src, size_t esz,
                              cudaMemcpyKind kind)
 {
     char *d = (char *)dst + ((size_t)(PADR - s->hn) * s->pitch + PADC) * esz;
+    const size_t rows = (size_t)(s->cfg.nrows + s->hn + s->hs);
+    if (kind == cudaMemcpyHostToDevice)
+        return fcab::h2d_rows(d, (size_t)s->pitch * esz, src, (size_t)s->cfg.ncols * esz, rows,
+                              s->stream);
     return cudaMemcpy2DAsync(d, (size_t)s->pitch * esz, src, (size_t)s->cfg.ncols * esz,
-                             (size_t)s->cfg.ncols * esz, (size_t)(s->cfg.nrows + s->hn + s->hs),
-                             kind, s->stream);
+                             (size_t)s->cfg.ncols * esz, rows, kind, s->stream);
 }
 
 static cudaError_t get_field(FcabSim *s, void *dst, const void *src, size_t esz)
 {
     const char *sp = (const char *)src + ((size_t)PADR * s->pitch + PADC) * esz;
-    return cudaMemcpy2DAsync(dst, (size_t)s->cfg.ncols * esz, sp, (size_t)s->pitch * esz,
-                             (size_t)s->cfg.ncols * esz, (size_t)s->cfg.nrows,
-                             cudaMemcpyDeviceToHost, s->stream);
+    return fcab::d2h_rows(dst, sp, (size_t)s->pitch * esz, (size_t)s->cfg.ncols * esz,
+                          (size_t)s->cfg.nrows, s->stream);
 }
 
 static int fill_interior(FcabSim *s, void *dst, double v)
@@ -344,7 +346,7 @@ static int rebuild_rain(FcabSim *s)
     unsigned long long init[2] = {~0ull, 0ull};
     CUDA_TRY(cudaMemcpyAsync(s->scratch, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
     if (!s->cr)
-        CUDA_TRY(cudaMalloc(&s->cr, s->nelem * s->esize));
+        CUDA_TRY(fcab::cached_malloc(&s->cr, s->nelem * s->esize));
     CUDA_TRY(cudaMemsetAsync(s->cr, 0, s->nelem * s->esize, s->stream));
     const int nb = 1024;
     if (s->esize == 8)
@@ -416,9 +418,9 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
         CUDA_TRY(put_field(s, s->tmax, tmax, es, kind));
     // staging copies of C and Rday for the rain field
     if (!s->tmpC)
-        CUDA_TRY(cudaMalloc(&s->tmpC, s->nelem * es));
+        CUDA_TRY(fcab::cached_malloc(&s->tmpC, s->nelem * es));
     if (!s->tmpR)
-        CUDA_TRY(cudaMalloc(&s->tmpR, s->nelem * es));
+        CUDA_TRY(fcab::cached_malloc(&s->tmpR, s->nelem * es));
     CUDA_TRY(cudaMemsetAsync(s->tmpC, 0, s->nelem * es, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->tmpR, 0, s->nelem * es, s->stream));
     if (C)

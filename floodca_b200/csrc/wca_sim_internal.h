@@ -48,4 +48,19 @@ namespace fcab {
 void set_error(const char *msg);
 // Run constants of an FP32 configuration (defined in wca_sim.cu).
 void make_run_params_f32(const FcabConfig &cfg, RunK<float> *rk, TimeCfg *tc);
+// Row-block copies between dense pageable host rows and pitched device rows
+// through pinned staging buffers and several host threads (host_copy.cu).
+// h2d_rows returns once the host rows have been read (the transfer may still
+// run; later work on `stream` follows it); d2h_rows returns with the host
+// rows written.
+cudaError_t h2d_rows(void *dst, size_t dpitch, const void *src, size_t row_bytes, size_t rows,
+                     cudaStream_t stream);
+cudaError_t d2h_rows(void *dst, const void *src, size_t spitch, size_t row_bytes, size_t rows,
+                     cudaStream_t stream);
+// Caching allocator of session buffers (mem_cache.cu): freed blocks are kept
+// per device for the next request of about the same size. A block must be
+// idle (its stream synchronised) when it is freed.
+cudaError_t cached_malloc(void **p, size_t bytes);
+cudaError_t cached_malloc_host(void **p, size_t bytes);
+void cached_free(void *p);
 }  // namespace fcab

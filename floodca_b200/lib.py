@@ -62,6 +62,7 @@ def core() -> C.CDLL:
                                              C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
         "fcab_sim_launches": (C.c_longlong, [_P]),
         "fcab_sim_stream": (_P, [_P]),
+        "fcab_release_cached_memory": (None, []),
         "fcab_sim_set_slab": (C.c_int, [_P, _I, _I]),
         "fcab_sim_slab_step": (C.c_int, [_P]),
         "fcab_sim_slab_vfull": (C.c_int, [_P]),

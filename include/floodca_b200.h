@@ -282,6 +282,12 @@ FCAB_API int fcab_sim_count_flooded(FcabSim *s, int nthr, const double *thr, uin
 /* The session's cudaStream_t. */
 FCAB_API void *fcab_sim_stream(FcabSim *s);
 
+/* Session buffers freed by fcab_sim_destroy (and by fca_cuda_run, which
+ * destroys its session on return) are kept on their device for the next
+ * session of about the same size, up to FCAB_CACHE_BYTES (environment;
+ * default a quarter of the device memory; 0 disables). This frees them. */
+FCAB_API void fcab_release_cached_memory(void);
+
 /* ---- Slabs of a row-split domain (the reference's distributed run:
  * owned rows [r0, r1) of FcaGrid, src/common/fca_types.h:103-104, with
  * comm->halo and comm->min_real, src/common/model.c:143-144,359-360,

@@ -18,8 +18,9 @@ own OpenMP core (compiled from its sources with its release flags) on a
 bounded sample of the same workload on this host's cores.
 
 --impl reference times that reference CPU implementation alone.
-Multi-GPU: independent replicas, one per rank (the single-domain path has no
-exchange step); value is the whole-job aggregate, max-over-ranks time.
+Multi-GPU: independent replicas, one per rank (the 4096^2 domain fits one
+GPU; domains beyond one GPU run as row slabs, floodca_b200.slabs); value is
+the whole-job aggregate, max-over-ranks time.
 """
 from __future__ import annotations
 

@@ -565,6 +565,38 @@ __device__ __forceinline__ StepVals<T> step_vals(const GridD<T> &g, const RunK<T
     return v;
 }
 
+// The next-step velocity of one flagged cell given its largest level
+// differences to orthogonal (mo) and diagonal (md) neighbours: a cheap upper
+// bound first, the exact velocity only when it could raise the running
+// maximum (FloodCA src/kernels/physics.h:158-217 for the formulas).
+template <typename T, int K, int MATH>
+__device__ __forceinline__ T dt_cell(T hv, T nv, T mo, T md, const StepK<T> &k, T dd, T vmax,
+                                     T vseed)
+{
+    T Sb = mo * k.rdx;
+    if constexpr (K == 8) {
+        const T sd = md * k.rdd;
+        Sb = sd > Sb ? sd : Sb;
+    }
+    if (cell_velocity_bound<T>(hv, nv, Sb * T(1.000001), k) <= (vmax > vseed ? vmax : vseed))
+        return vmax;
+    T Smax = Mth<T, MATH>::div(mo, k.dx);
+    if constexpr (K == 8) {
+        const T Sd = Mth<T, MATH>::div(md, dd);
+        if (Sd > Smax)
+            Smax = Sd;
+    }
+    const T v = cell_velocity<T, MATH>(hv, nv, Smax, k);
+    return v > vmax ? v : vmax;
+}
+
+template <typename T, int K, int MATH>
+__device__ __noinline__ T dt_cell_out(T hv, T nv, T mo, T md, const StepK<T> k, T dd, T vmax,
+                                      T vseed)
+{
+    return dt_cell<T, K, MATH>(hv, nv, mo, md, k, dd, vmax, vseed);
+}
+
 // A warp's running sums over the cells it writes.
 template <typename T, typename AccT>
 struct StepSums {
@@ -1017,25 +1049,13 @@ __device__ __forceinline__ void sweep_segment(const GridD<T> &g, const RunK<T> &
                     md = fmax(md, fabs(la - right_of<T, CPL>(L4, j, L4r)));
                     md = fmax(md, fabs(la - left_of<T, CPL>(L4, j, L4l)));
                 }
-                // cheap upper bound first; the exact velocity only when
-                // it could raise the running maximum
-                T Sb = mo * k.rdx;
-                if constexpr (K == 8) {
-                    const T sd = md * k.rdd;
-                    Sb = sd > Sb ? sd : Sb;
-                }
-                if (cell_velocity_bound<T>(hv, p3.n[j], Sb * T(1.000001), k) <=
-                    (vmax > vseed ? vmax : vseed))
-                    continue;
-                T Smax = Mth<T, MATH>::div(mo, k.dx);
-                if constexpr (K == 8) {
-                    const T Sd = Mth<T, MATH>::div(md, dd);
-                    if (Sd > Smax)
-                        Smax = Sd;
-                }
-                const T v = cell_velocity<T, MATH>(hv, p3.n[j], Smax, k);
-                if (v > vmax)
-                    vmax = v;
+                // K = 8 evaluates the cell out of line: fewer live registers
+                // in the sweep (measured 3 % faster for K = 8 at 4096^2 on a
+                // B200, 6 % slower for K = 4)
+                if constexpr (K == 8)
+                    vmax = dt_cell_out<T, K, MATH>(hv, p3.n[j], mo, md, k, dd, vmax, vseed);
+                else
+                    vmax = dt_cell<T, K, MATH>(hv, p3.n[j], mo, md, k, dd, vmax, vseed);
             }
         }
 

@@ -53,19 +53,23 @@ cudaError_t ensure(Pool &p)
 {
     if (p.ready)
         return cudaSuccess;
+    // resources made by an earlier, failed attempt are kept and not remade
     cudaError_t e;
     p.n = workers_wanted();
-    if ((e = cudaEventCreateWithFlags(&p.start, cudaEventDisableTiming)) != cudaSuccess)
+    if (!p.start && (e = cudaEventCreateWithFlags(&p.start, cudaEventDisableTiming)) != cudaSuccess)
         return e;
     for (int i = 0; i < p.n; i++) {
         Worker &w = p.w[i];
-        if ((e = cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) != cudaSuccess)
+        if (!w.st && (e = cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
-        for (int k = 0; k < 2; k++)
-            if ((e = cudaMallocHost(&w.slot[k], SLOT)) != cudaSuccess ||
-                (e = cudaEventCreateWithFlags(&w.ev[k], cudaEventDisableTiming)) != cudaSuccess)
+        if (!w.done && (e = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+        for (int k = 0; k < 2; k++) {
+            if (!w.slot[k] && (e = cudaMallocHost(&w.slot[k], SLOT)) != cudaSuccess)
                 return e;
+            if (!w.ev[k] && (e = cudaEventCreateWithFlags(&w.ev[k], cudaEventDisableTiming)) != cudaSuccess)
+                return e;
+        }
     }
     p.ready = true;
     return cudaSuccess;

@@ -1235,12 +1235,21 @@ struct BatchQ {
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128, CPL == 2 ? 3 : 1)
+__global__ void __launch_bounds__(128, CPL == 2 ? 4 : 1)
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,
                                                     BatchQ *q, int *need_list)
 {
     const int lane = threadIdx.x & 31;
+    // The unit's member descriptor and step constants live in the warp's
+    // shared-memory slot, not in registers: the compiler reloads them where
+    // needed instead of holding ~60 warp-uniform values, which lets 4 CTAs
+    // (16 warps) fit per SM (measured on a B200, 64 config-4 members: 39.6
+    // against 37.1 G cell-steps/s with register copies at 3 CTAs).
+    const int wib = threadIdx.x >> 5;
+    __shared__ MemberD<T> smd[4];
+    __shared__ StepVals<T> ssv[4];
+    static_assert(sizeof(MemberD<T>) % 4 == 0 && sizeof(StepVals<T>) % 4 == 0, "word copies");
     for (;;) {
         unsigned u = 0;
         if (lane == 0)
@@ -1249,16 +1258,30 @@ k_step_batch(const MemberD<T> *members,
         if (u >= (unsigned)total_units)
             break;
         const int m = unit_member[u];
-        const MemberD<T> &md = members[m];
+        __syncwarp();
+        {
+            const unsigned *src = reinterpret_cast<const unsigned *>(members + m);
+            unsigned *dst = reinterpret_cast<unsigned *>(&smd[wib]);
+            for (int w = lane; w < (int)(sizeof(MemberD<T>) / 4); w += 32)
+                dst[w] = src[w];
+        }
+        __syncwarp();
+        const MemberD<T> &md = smd[wib];
         Ctl *ctl = md.ctl;
         if (ctl->active == 0)
             continue;
-        const GridD<T> g = md.g;
-        const RunK<T> rk = md.rk;
+        const GridD<T> &g = md.g;
+        const RunK<T> &rk = md.rk;
         const int local = (int)u - md.unit_off;
         const int strip = local % md.strips, blk = local / md.strips;
         const int r0 = blk * md.seg, r1 = min(g.nr, r0 + md.seg);
-        const StepVals<T> sv = step_vals<T, K>(g, rk, ctl);
+        {
+            const StepVals<T> sv0 = step_vals<T, K>(g, rk, ctl);
+            if (lane == 0)
+                ssv[wib] = sv0;
+        }
+        __syncwarp();
+        const StepVals<T> &sv = ssv[wib];
         StepSums<T, AccT> ss;
         sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
         publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, (int)(u & (NSLOT - 1)));

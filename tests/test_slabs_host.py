@@ -170,3 +170,16 @@ def test_toy_detects_a_missing_exchange():
             s.step()
     got = np.concatenate([s._own() for s in slabs])
     assert not np.array_equal(got, _toy_single(nr, nc, steps))
+
+
+def test_merge_stats_counts_inflow_once():
+    a = dict(t=10.0, dt_base=1.0, step=5, done=1, V=3.0, V0=1.0, V_rain=1.5, clamp_err=0.0,
+             V_sea=0.25, V_bnd=0.25, V_in=2.0, cap_active=3, cap_total=10, dt_min_hits=1,
+             E_mass=0.0, dt_full_passes=2)
+    b = dict(a, V=2.0, V0=0.5, V_rain=0.5, V_sea=0.0, V_bnd=0.0, cap_active=1, cap_total=6)
+    from floodca_b200.slabs import merge_stats
+    m = merge_stats([a, b], [False, True])          # b owns the inflow cell
+    assert (m["V"], m["V0"], m["V_rain"], m["cap_active"], m["cap_total"]) == (5.0, 1.5, 2.0, 4, 16)
+    assert m["V_in"] == 2.0 and (m["step"], m["t"], m["dt_min_hits"]) == (5, 10.0, 1)
+    # V + V_sea + V_bnd - V_rain - V_in - V0 = 5 + 0.5 - 2 - 2 - 1.5 = 0
+    assert m["E_mass"] == 0.0

@@ -128,7 +128,8 @@ extern "C" {
  * edges as open); a CUDA failure returns -2 instead of exit(1); a fixed-step
  * run (cfg->steps > 0) whose step would have dt <= 0 stops instead of
  * looping forever. Returns 0, -1 on a bad block shape (same check as the
- * reference), -2 on a device error. */
+ * reference), -2 on a device error. The run's device buffers stay cached
+ * for later runs (fcab_release_cached_memory frees them). */
 FCAB_API int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *tm);
 
 /* Replaces fca_cuda_device_name (src/cuda/kernels.cu:606-615). */

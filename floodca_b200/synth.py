@@ -127,3 +127,60 @@ def config3(seed: int = 3, n: int = 2048) -> tuple[Domain, RunParams]:
     """2048x2048 from the config-1 generator, 100 mm/h for 3 h, 6 h simulated."""
     dom = make_terrain(TerrainSpec(n, n, amplitude=5.0, seed=seed))
     return box_rain(dom, south_open().with_(T_sim=21600.0), 100.0, 3.0)
+
+
+# ---------------------------------------------------------------------------
+# The reference's grid directory (FloodCA src/common/grid.c:162-237,
+# src/common/io.c:34-56): dem.json {nrows, ncols, dx, dtype, x0, y0, ...}
+# and raw row-major float32 rasters dem.bin, n.bin, C.bin, Rday.bin, h.bin
+# plus uint8 mask.bin (row 0 = north). Missing optional rasters load as
+# n = 0.03, C = 0, Rday = 0, h = 0.
+
+def write_grid_dir(dom: Domain, path, name: str = "synthetic", x0: float = 0.0,
+                   y0: float = 0.0) -> None:
+    """Writes `dom` as a grid directory the reference's CLIs read (--grid)."""
+    import json
+    from pathlib import Path
+    d = Path(path)
+    d.mkdir(parents=True, exist_ok=True)
+    nr, nc = dom.shape
+    hdr = {"name": name, "nrows": int(nr), "ncols": int(nc), "dx": float(dom.dx),
+           "dtype": "float32", "crs": "EPSG:32643", "x0": float(x0), "y0": float(y0),
+           "nodata": -9999, "source": "floodca_b200.synth", "sha256": ""}
+    (d / "dem.json").write_text(json.dumps(hdr) + "\n")
+    for fname, arr in (("dem", dom.z), ("n", dom.n), ("C", dom.C), ("Rday", dom.Rday),
+                       ("h", dom.h)):
+        np.ascontiguousarray(arr, np.float32).tofile(d / f"{fname}.bin")
+    np.ascontiguousarray(dom.mask, np.uint8).tofile(d / "mask.bin")
+
+
+def read_grid_dir(path) -> Domain:
+    """Reads a grid directory as the reference's fca_grid_load_dir does."""
+    import json
+    from pathlib import Path
+    d = Path(path)
+    hdr = json.loads((d / "dem.json").read_text())
+    nr, nc, dx = int(hdr["nrows"]), int(hdr["ncols"]), float(hdr.get("dx", 30.0))
+
+    def f32(name, default):
+        p = d / f"{name}.bin"
+        if p.exists():
+            return np.fromfile(p, np.float32, nr * nc).reshape(nr, nc)
+        return np.full((nr, nc), default, np.float32)
+
+    h = f32("h", None) if (d / "h.bin").exists() else f32("h0", 0.0)
+    return Domain(z=f32("dem", 0.0), mask=np.fromfile(d / "mask.bin", np.uint8, nr * nc).reshape(nr, nc),
+                  n=f32("n", 0.03), C=f32("C", 0.0), Rday=f32("Rday", 0.0), h=h, dx=dx)
+
+
+def read_field(path, name: str, shape) -> np.ndarray:
+    """An output raster (hmax, h_final) the reference writes with
+    fca_grid_write_field (float32, or float64 when its JSON says so)."""
+    import json
+    from pathlib import Path
+    d = Path(path)
+    dt = np.float32
+    j = d / f"{name}.json"
+    if j.exists() and json.loads(j.read_text()).get("dtype") == "float64":
+        dt = np.float64
+    return np.fromfile(d / f"{name}.bin", dt).reshape(shape)

@@ -49,6 +49,10 @@ def build(ref_root: str = "/root/reference") -> bool:
         return False
     subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}", "-j4"],
                    check=True)
+    # the reference's CUDA CLI linked against the drop-in library, once it is built
+    if (ROOT / "floodca_b200" / "libfloodca_b200.so").exists():
+        subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}",
+                        "dropin"], check=True)
     return True
 
 

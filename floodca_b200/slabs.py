@@ -93,13 +93,16 @@ class _DevWords:
 
 
 class Slab(Session):
-    """The session of one slab: own rows plus halo rows of its neighbours."""
+    """The session of one slab: own rows plus halo rows of its neighbours.
+    `vmax` is a device view (int64) of the session's pending velocity
+    maximum, valid while the slab is open."""
 
     def __init__(self, dom: Domain, p: RunParams, spec: SlabSpec, precision: str = "f32",
                  math: str = "exact", cols_per_lane: int = 0, seg_rows: int = 0, stream=None):
         d, q = slab_domain(dom, p, spec)
         self.spec = spec
-        self.owns_inflow = p.inflow_cell >= 0 and spec.r0 <= p.inflow_cell // dom.shape[1] < spec.r1
+        row_in = p.inflow_cell // dom.shape[1]
+        self.owns_inflow = p.inflow_cell >= 0 and spec.r0 <= row_in < spec.r1
         self.dom = d.astype(np.float64 if precision == "f64" else np.float32)
         self._create(SimpleNamespace(shape=(spec.rows, dom.shape[1]), dx=dom.dx), q, precision,
                      math, cols_per_lane, seg_rows, stream)

@@ -201,6 +201,14 @@ class Session:
               "fcab_sim_count_flooded")
         return [int(v) for v in fl], float(mx.value)
 
+    def write_outputs(self, out_dir) -> None:
+        """hmax and h_final in the reference's output format, as its CLIs
+        write them (src/cuda/main_cuda.c:73-80)."""
+        from .synth import write_field
+        h, hmax, _ = self.download()
+        write_field(out_dir, "hmax", hmax, self.cfg.dx)
+        write_field(out_dir, "h_final", h, self.cfg.dx)
+
     def launches(self) -> int:
         return int(self.L.fcab_sim_launches(self.h))
 

@@ -184,3 +184,24 @@ def read_field(path, name: str, shape) -> np.ndarray:
     if j.exists() and json.loads(j.read_text()).get("dtype") == "float64":
         dt = np.float64
     return np.fromfile(d / f"{name}.bin", dt).reshape(shape)
+
+
+def write_field(path, name: str, arr: np.ndarray, dx: float, x0: float = 0.0,
+                y0: float = 0.0) -> None:
+    """Writes an output raster (hmax, h_final, ...) as the reference's
+    fca_grid_write_field does (src/common/grid.c:271-306): <name>.bin, raw
+    float32 (float64 for a float64 array, the FCA_DOUBLE build), and a
+    <name>.json header with the grid's shape, dx, dtype, CRS and origin."""
+    import json
+    import time
+    from pathlib import Path
+    d = Path(path)
+    d.mkdir(parents=True, exist_ok=True)
+    a = np.ascontiguousarray(arr, np.float64 if arr.dtype == np.float64 else np.float32)
+    a.tofile(d / f"{name}.bin")
+    nr, nc = a.shape
+    hdr = {"name": name, "nrows": int(nr), "ncols": int(nc), "dx": float(np.float32(dx)),
+           "dtype": "float64" if a.dtype == np.float64 else "float32", "crs": "EPSG:32643",
+           "x0": float(x0), "y0": float(y0), "nodata": -9999, "source": "floodca",
+           "created": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()), "sha256": ""}
+    (d / f"{name}.json").write_text(json.dumps(hdr, separators=(",", ":")) + "\n")

@@ -51,3 +51,13 @@ def test_reference_cli_runs_on_the_dropin(tmp_path, kind, K, U):
         # libm) are both faithfully rounded but may differ in the last bit
         for a, b in ((hmax, ref["hmax"]), (h, ref["h"])):
             assert np.abs(a - b).max() <= 1e-12
+
+    # the Python API's session on the same grid writes the same output files
+    from floodca_b200.sim import Session
+    with Session(synth.read_grid_dir(grid), p, precision=kind) as sess:
+        sess.run()
+        sess.write_outputs(tmp_path / "mine")
+    for name in ("hmax", "h_final"):
+        mine = synth.read_field(tmp_path / "mine", name, d.shape)
+        assert mine.dtype == hmax.dtype
+        assert np.array_equal(mine, synth.read_field(out, name, d.shape)), name

@@ -63,3 +63,31 @@ def test_reference_loader_defaults_for_missing_rasters(tmp_path):
     back = synth.read_grid_dir(tmp_path / "g")
     for k, v in (("n", 0.03), ("C", 0.0), ("Rday", 0.0), ("h", 0.0)):
         assert np.all(r[k] == np.float32(v)) and np.array_equal(getattr(back, k), r[k]), k
+
+
+@pytest.mark.parametrize("kind", ["f32", "f64"])
+def test_output_field_matches_reference_writer(tmp_path, kind):
+    """synth.write_field writes the same raster bytes and header fields as
+    the reference's fca_grid_write_field (src/common/grid.c:271-306)."""
+    import json
+    L = refcore.lib(kind)
+    dbl = kind == "f64"
+    T = abi.fca_types(C.c_double if dbl else C.c_float)
+    L.fca_grid_write_field.restype = C.c_int
+    L.fca_grid_write_field.argtypes = [C.POINTER(T.FcaGrid), C.c_char_p, C.c_char_p,
+                                       C.POINTER(T.real)]
+    rng = np.random.default_rng(2)
+    arr = rng.uniform(0, 3, (11, 7)).astype(np.float64 if dbl else np.float32)
+    g = T.FcaGrid()
+    g.nrows, g.ncols, g.dx, g.x0, g.y0 = 11, 7, 90.0, 500000.0, 1450000.0
+    ref_dir, my_dir = tmp_path / "ref", tmp_path / "mine"
+    ref_dir.mkdir()
+    assert L.fca_grid_write_field(C.byref(g), str(ref_dir).encode(), b"hmax",
+                                  arr.ctypes.data_as(C.POINTER(T.real))) == 0
+    synth.write_field(my_dir, "hmax", arr, 90.0, 500000.0, 1450000.0)
+    assert (my_dir / "hmax.bin").read_bytes() == (ref_dir / "hmax.bin").read_bytes()
+    a = json.loads((ref_dir / "hmax.json").read_text())
+    b = json.loads((my_dir / "hmax.json").read_text())
+    a.pop("created"), b.pop("created")
+    assert a == b
+    assert np.array_equal(synth.read_field(my_dir, "hmax", arr.shape), arr)

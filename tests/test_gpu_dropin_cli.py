@@ -62,21 +62,3 @@ def test_reference_cli_runs_on_the_dropin(tmp_path, kind, K, U):
         assert mine.dtype == hmax.dtype
         assert np.array_equal(mine, synth.read_field(out, name, d.shape)), name
 
-
-def test_python_cli_matches_reference_core(tmp_path):
-    """`python -m floodca_b200` with the reference CLI's options (and the
-    per-edge extension) writes the reference CPU core's hmax, bit for bit."""
-    from floodca_b200 import cli
-    if not refcore.available("f32"):
-        pytest.skip("the reference core is built with the reference sources")
-    d = synth.make_terrain(synth.TerrainSpec(64, 48, seed=5))
-    d.h = np.full(d.shape, 0.02, np.float32)
-    d.Rday = np.full(d.shape, 0.48, np.float32)
-    synth.write_grid_dir(d, tmp_path / "grid")
-    rc = cli.main(["--grid", str(tmp_path / "grid"), "--tsim", "1800", "--hyeto", "uniform",
-                   "--neigh", "8", "--edges", "0100", "--out", str(tmp_path / "out")])
-    assert rc == 0
-    p = RunParams(K=8, hyeto="uniform", T_sim=1800.0, edges=(0, 1, 0, 0))
-    ref = refcore.run(synth.read_grid_dir(tmp_path / "grid"), p, kind="f32")
-    assert np.array_equal(synth.read_field(tmp_path / "out", "hmax", d.shape), ref["hmax"])
-    assert np.array_equal(synth.read_field(tmp_path / "out", "h_final", d.shape), ref["h"])

@@ -1,6 +1,6 @@
 """Throughput of the fused WCA flood step on B200.
 
-Workload: a 4096 x 4096 grid at 90 m (16.8 M LAND
+Workload (config 2 of the benchmark set): a 4096 x 4096 grid at 90 m (16.8 M LAND
 cells), fBm relief of 20 m amplitude, six Manning classes, 30 mm/h rain for
 2 h and a north-edge point inflow (triangle peaking at 500 m^3/s at 3 h),
 open south edge. A "step" is one WCA step over the whole grid. The timed

@@ -1,4 +1,5 @@
-"""Batched ensembles of WCA runs and their baseline.
+"""Batched ensembles of WCA runs (config 4: 256 members of side 512-2048) and
+their one-at-a-time baseline.
 
 Config 4: members of side drawn uniformly from 512..2048 (multiples of 64),
 each with its own seeded terrain (the config-1 generator), Manning n scaled

@@ -1,4 +1,4 @@
-"""Precision study on the GPU.
+"""Precision study (config 3: 2048 x 2048, three precisions) on the GPU.
 
 The 2048 x 2048 config-1-generator grid (100 mm/h for 3 h, 6 h simulated)
 runs three ways with the same kernel family:

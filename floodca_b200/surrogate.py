@@ -1,4 +1,4 @@
-"""Surrogate-screened flood ensembles.
+"""Surrogate-screened flood ensembles (config 5: 10,000 members of 256 x 256).
 
 Members are 256 x 256 grids of the config-4 generator (own terrain, Manning
 n x lognormal(0, 0.3), uniform rain of 20-150 mm/h for 0.5-4 h, 8 h

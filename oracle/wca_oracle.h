@@ -38,7 +38,7 @@ typedef struct OrParams {
     double T_sim, out_every;
     int hyeto;                        /* 0 triangle, 1 uniform */
     double D_h, phi, lambda;
-    /* Extensions without a reference counterpart (documented in DESIGN.md):
+    /* Extensions without a reference counterpart:
      * rain_end > 0 makes the rain source zero for steps starting at
      * t >= rain_end and adds rain_end as a step event; inflow_cell >= 0 adds a
      * triangular point hydrograph (0 at t=0, peak at inflow_t_peak, 0 at

@@ -7,7 +7,8 @@ Outputs (next to this file):
 
 Run `python -m floodca_b200.build` (or `__graft_entry__.build()`). Objects
 go to _build/ at the repository root. Sources are rebuilt only when newer
-than their object.
+than their object. FCAB_NVCC_FLAGS adds nvcc flags (for example the launch
+shape macro -DFCAB_PAIR_WARPS=12); changing it needs a clean _build/.
 """
 from __future__ import annotations
 
@@ -30,7 +31,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # parity build does on the host (-ffp-contract=off); explicit fmaf() calls
 # in the kernels are unaffected.
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC)]
+           "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC),
+           *os.environ.get("FCAB_NVCC_FLAGS", "").split()]
 
 CORE_SRCS = ["wca_inst_f32.cu", "wca_inst_f32all.cu", "wca_inst_f64.cu", "wca_inst_batch.cu",
              "wca_sim.cu", "host_copy.cu", "mem_cache.cu", "wca_noalloc.cu", "wca_batch.cu", "unet_tc.cu"]

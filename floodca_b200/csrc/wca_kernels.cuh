@@ -35,7 +35,8 @@
 
 namespace fcab {
 
-constexpr int PADR = 4;   // padded rows above and below the grid
+constexpr int PADR = 8;   // padded rows above and below the grid (the pair sweep
+                          // starts up to six rows above a segment)
 constexpr int PADC = 4;   // padded columns left of the grid
 constexpr int NSLOT = 32; // accumulator slots (spread the atomics)
 constexpr double PAD_Z = 1e30;   // padding elevation of all-LAND grids
@@ -83,7 +84,7 @@ struct Ctl {
     int step, hit, active, h_cur, want_v, done, pause, force_day;
     int err, n_force_days;
     int fin_pending;            // slab runs: 1 after a step, 2 after the first velocity pass
-    int pad1;
+    int inflow_off;             // 1: the inflow cell is not LAND (no inflow volume)
     long long dt_min_hits;
     unsigned long long vmax_bits;
     unsigned int ctas_done;
@@ -301,7 +302,7 @@ __device__ void finalize(Ctl *c, const TimeCfg &tc, const RunK<T> &rk, bool afte
     if (!done) {
         bool rain_on = tc.rain_end <= 0.0 || tc.rain_end - t >= 1e-9;
         F = rain_on ? hyeto_integral(tc, t, (double)dt) : 0.0;
-        V_in = inflow_volume(tc, t, (double)dt);
+        V_in = c->inflow_off ? 0.0 : inflow_volume(tc, t, (double)dt);
     }
     c->t = t;
     c->step = step;
@@ -1135,6 +1136,20 @@ __device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVa
     }
 }
 
+}  // namespace fcab
+
+#include "wca_sweep_f2.cuh"
+
+namespace fcab {
+
+// The pair sweep runs the FP32 all-LAND grids at two columns per lane;
+// every other variant runs sweep_segment.
+template <typename T, int CPL, bool LANDONLY>
+__host__ __device__ constexpr bool use_pair_sweep()
+{
+    return sizeof(T) == 4 && CPL == 2 && LANDONLY;
+}
+
 // Launch shape of the step kernel: threads per CTA and the resident warps
 // per SM the register allocation aims for (65536 / (32 x warps) registers
 // per thread). Measured at 4096^2 on a B200: the exact CPL-2 kernel runs 15 %
@@ -1147,12 +1162,12 @@ __device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVa
 #define FCAB_STEP_WARPS 0
 #endif
 template <int CPL, int MATH>
-constexpr int step_threads()
+__host__ __device__ constexpr int step_threads()
 {
     return FCAB_STEP_THREADS;
 }
 template <int K, int CPL, int MATH>
-constexpr int step_min_blocks()
+__host__ __device__ constexpr int step_min_blocks()
 {
     // K = 8 exact at CPL 2 spills 56 B at 16 warps and runs 3.5 % faster at 12
     return (FCAB_STEP_WARPS > 0
@@ -1161,9 +1176,21 @@ constexpr int step_min_blocks()
                             : CPL == 2 ? (MATH == MATH_EXACT && K == 4 ? 16 : 12) : 8)) /
            (step_threads<CPL, MATH>() / 32);
 }
+// Resident warps per SM the pair sweep's register allocation aims for: at 8
+// (up to 255 registers) its four-row ring of packed pairs needs no spills.
+#ifndef FCAB_PAIR_WARPS
+#define FCAB_PAIR_WARPS 8
+#endif
+template <typename T, int K, int CPL, int MATH, bool LANDONLY>
+__host__ __device__ constexpr int step_blocks_per_sm()
+{
+    return use_pair_sweep<T, CPL, LANDONLY>() ? FCAB_PAIR_WARPS / (step_threads<CPL, MATH>() / 32)
+                                              : step_min_blocks<K, CPL, MATH>();
+}
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(step_threads<CPL, MATH>(), step_min_blocks<K, CPL, MATH>()) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
+__global__ void __launch_bounds__(step_threads<CPL, MATH>(),
+                                  step_blocks_per_sm<T, K, CPL, MATH, LANDONLY>()) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
                                               int warps_total)
 {
     using G = Geom<CPL>;
@@ -1181,12 +1208,23 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(), step_min_blocks<K, 
     if (wid >= warps_total)
         w0 = w1 = 0;
 
+    // step constants in shared memory for the pair sweep's exact re-evaluations
+    __shared__ StepK<T> sk;
+    if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+        if (threadIdx.x == 0)
+            sk = sv.k;
+        __syncthreads();
+    }
     while (w0 < w1) {
         const int strip = (int)(w0 / nr);
         const int r0 = (int)(w0 % nr);
         const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
         w0 += r1 - r0;
-        sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
+        if constexpr (use_pair_sweep<T, CPL, LANDONLY>())
+            PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &sk, strip, r0, r1, lane, ss);
+        else
+            sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane,
+                                                                  ss);
     }
 
     publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, wid & (NSLOT - 1));
@@ -1235,7 +1273,8 @@ struct BatchQ {
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128, CPL == 2 ? 4 : 1)
+__global__ void __launch_bounds__(128, use_pair_sweep<T, CPL, LANDONLY>() ? FCAB_PAIR_WARPS / 4
+                                                                      : (CPL == 2 ? 4 : 1))
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,
                                                     BatchQ *q, int *need_list)
@@ -1283,7 +1322,11 @@ k_step_batch(const MemberD<T> *members,
         __syncwarp();
         const StepVals<T> &sv = ssv[wib];
         StepSums<T, AccT> ss;
-        sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane, ss);
+        if constexpr (use_pair_sweep<T, CPL, LANDONLY>())
+            PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &ssv[wib].k, strip, r0, r1, lane, ss);
+        else
+            sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane,
+                                                                  ss);
         publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, (int)(u & (NSLOT - 1)));
         if (lane == 0) {
             __threadfence();

@@ -1,0 +1,696 @@
+// The FP32 sweep on column pairs for all-LAND grids.
+//
+// Same work decomposition and the same arithmetic as sweep_segment (one warp
+// streams a strip of 64 columns down a range of rows; iteration i loads row
+// i+1 and runs A faces of rows i-1/i, C limiter of row i-1, D update of row
+// i-2, E next-step velocity of row i-3; FloodCA src/kernels/physics.h and
+// src/common/model.c:321-605), organised for instruction count:
+//
+//  * a lane's two columns are one packed f32x2 register pair, so every add,
+//    multiply and fused multiply-add runs on both columns in one instruction
+//    (the same rounding per half as the scalar instruction);
+//  * the iteration body is unrolled four times over ring-indexed registers
+//    (row r lives in slot (r - i0) & 3), so the pipeline never copies
+//    registers from one row to the next;
+//  * the exact formulas run optimistically: each face takes the common path
+//    (no critical-velocity cap, no volume cap, a cube root whose rounding is
+//    decided) and flags the halves where that is not certain; a warp with a
+//    flagged half re-evaluates those halves with the exact scalar formula
+//    (face_q). The same holds for the limiter (a division only where the
+//    outflow exceeds the held volume), the clamp and the next-step velocity
+//    (a multiply-only bound h^4 S^3 >= thr^6 n^6 before the exact value);
+//  * the upwind-scaled discharge of every face is formed once, as
+//    Q- * s_down + Q+ * s_up with Q+ = max(Q, 0), Q- = min(Q, 0) (one of the
+//    two products is zero, so this is the reference's Q * s_upwind), and
+//    used by both cells of the face;
+//  * grid edges, open boundaries, the inflow cell and rows outside the grid
+//    are handled in warp-uniform branches that only edge strips and edge
+//    rows take.
+#pragma once
+
+#include "wca_f2.cuh"
+
+namespace fcab {
+
+// Packed per-step constants of the pair sweep.
+struct PairK {
+    f2 dx, rdx, dd, rdd, w, A, invA, g, dt, rain, half, nmin, vcrK, capK;
+    float tau_l, tau_h;
+};
+
+__device__ __forceinline__ f2 ld2(const float *p)
+{
+    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    return mk2(v.x, v.y);
+}
+__device__ __forceinline__ f2 ld2_rw(const float *p)
+{
+    const float2 v = *reinterpret_cast<const float2 *>(p);
+    return mk2(v.x, v.y);
+}
+__device__ __forceinline__ void st2(float *p, f2 v)
+{
+    *reinterpret_cast<float2 *>(p) = make_float2(lo2(v), hi2(v));
+}
+
+// Discharge a -> b of two faces (one per half) between all-LAND cells with
+// old levels La, Lb, elevations za, zb and Manning n na, nb, centre distance
+// d (rd = RN(1/d)) and width w (FloodCA src/kernels/physics.h:51-125).
+// MATH_EXACT: the common path; `un0`/`un1` flag live halves whose value the
+// exact scalar formula must settle (cube root near a rounding midpoint or
+// out of range, velocity near or above the critical velocity, volume cap
+// possibly binding). MATH_FAST: hardware approximations throughout, volume
+// cap applied; `un*` then flag capped halves (for the cap count).
+template <int MATH>
+__device__ __forceinline__ f2 face2(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2 d, f2 rd, f2 w,
+                                    const PairK &c, bool &un0, bool &un1)
+{
+    const f2 dL = sub2(La, Lb);
+    const f2 Lmx = max2(La, Lb);
+    const f2 adL = sub2(Lmx, min2(La, Lb));        // |dL|, the same rounding
+    const f2 hf = sub2(Lmx, max2(za, zb));
+    float a0, a1, h0, h1;
+    sp2(adL, a0, a1);
+    sp2(hf, h0, h1);
+    const bool live0 = a0 >= c.tau_l && h0 >= c.tau_h;
+    const bool live1 = a1 >= c.tau_l && h1 >= c.tau_h;
+    const f2 nf = max2(mul2(c.half, add2(na, nb)), c.nmin);
+    f2 Qm;
+    if constexpr (MATH == MATH_EXACT) {
+        const f2 rnf = rcp2_nr(nf);
+        const f2 sq = sqrt2_nr(div2_mk(adL, d, rd));
+        bool s0, s1;
+        const f2 cb = cbrt_sq2(hf, s0, s1);
+        const f2 v = mul2(mul2(rnf, cb), sq);
+        const f2 v2 = mul2(v, v);
+        const f2 pm = mul2(mul2(c.g, hf), c.vcrK);
+        Qm = mul2(mul2(v, hf), w);
+        const f2 qc = mul2(adL, c.capK);             // below the exact volume cap
+        float v20, v21, p0, p1, q0, q1, m0, m1;
+        sp2(v2, v20, v21);
+        sp2(pm, p0, p1);
+        sp2(qc, q0, q1);
+        sp2(Qm, m0, m1);
+        un0 = live0 && (s0 || !(v20 < p0) || !(q0 > m0));
+        un1 = live1 && (s1 || !(v21 < p1) || !(q1 > m1));
+    } else {
+        const f2 rnf = rcp_2(nf);
+        const f2 S = mul2(adL, rd);
+        const f2 sq = mul2(S, rsqrt_2(S));
+        const f2 cb = ex2_2(mul2(lg2_2(hf), bc2(0.666666687f)));
+        f2 v = mul2(mul2(rnf, cb), sq);
+        const f2 p = mul2(c.g, hf);
+        const f2 vcr = mul2(p, rsqrt_2(p));
+        const f2 v2 = mul2(v, v);
+        v = sel2(lo2(v2) > lo2(p), hi2(v2) > hi2(p), vcr, v);
+        Qm = mul2(mul2(v, hf), w);
+        const f2 Qc = mul2(mul2(adL, c.A), c.capK);
+        const bool c0 = lo2(Qc) < lo2(Qm), c1 = hi2(Qc) < hi2(Qm);
+        Qm = sel2(c0, c1, Qc, Qm);
+        un0 = live0 && c0;
+        un1 = live1 && c1;
+    }
+    const f2 Q = copysign2(Qm, dL);
+    return sel2(live0, live1, Q, bc2(0.0f));
+}
+
+// Exact re-evaluation of the flagged halves of a face pair with the scalar
+// formula (face_q); `cap` counts the volume caps among them. The step
+// constants come through a pointer (shared memory) so that no register of
+// the caller has to live in memory around the call.
+struct Settled {
+    f2 Q;
+    unsigned cap;
+};
+
+static __device__ __noinline__ Settled face2_settle(f2 Q, bool un0, bool un1, f2 za, f2 ha, f2 na,
+                                                    f2 zb, f2 hb, f2 nb, bool diag,
+                                                    const StepK<float> *kp)
+{
+    const StepK<float> k = *kp;
+    const float d = diag ? k.d_diag : k.dx, rd = diag ? k.rdd : k.rdx;
+    Settled o;
+    o.cap = 0u;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 0 ? un0 : un1) {
+            int cap = 0;
+            const float q = face_q<float, MATH_EXACT>(get2(za, j), get2(ha, j), get2(na, j), M_LAND,
+                                                      get2(zb, j), get2(hb, j), get2(nb, j), M_LAND,
+                                                      d, rd, k, cap);
+            put2(Q, j, q);
+            o.cap += (unsigned)cap;
+        }
+    }
+    o.Q = Q;
+    return o;
+}
+
+// The exact next-step velocity of the flagged halves (physics.h:193-217),
+// folded into the running maximum vm.
+template <int K, int MATH>
+__device__ __noinline__ float pair_velocity(float vm, bool x0, bool x1, f2 mo, f2 md, f2 hv, f2 nv,
+                                            const StepK<float> *kp)
+{
+    const StepK<float> k = *kp;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 0 ? x0 : x1) {
+            float Smax = Mth<float, MATH>::div(get2(mo, j), k.dx);
+            if constexpr (K == 8) {
+                const float Sd = Mth<float, MATH>::div(get2(md, j), k.d_diag);
+                Smax = Sd > Smax ? Sd : Smax;
+            }
+            const float v = cell_velocity<float, MATH>(get2(hv, j), get2(nv, j), Smax, k);
+            vm = v > vm ? v : vm;
+        }
+    }
+    return vm;
+}
+
+// Open-edge faces of a row's two cells (model.c:442-479): discharge to the
+// virtual neighbour, clipped at zero; `add` is what each cell adds to its
+// outflow (the sum of its open slots, model.c:235-236), `ko` the open sides
+// (4 bits per cell, one per side), `cap` the volume caps of owned cells.
+struct OpenFaces {
+    f2 qo, add;
+    unsigned ko, cap;
+};
+
+static __device__ __noinline__ OpenFaces open_faces2(f2 z, f2 h, f2 n, int r, int cbase, int nr,
+                                                     int nc, int r_lo, int r_hi, int edges,
+                                                     bool own0, bool own1,
+                                                     const StepK<float> *kp)
+{
+    const StepK<float> k = *kp;
+    OpenFaces o;
+    o.ko = 0u;
+    o.cap = 0u;
+    float q[2] = {0.0f, 0.0f}, a[2] = {0.0f, 0.0f};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int cc = cbase + j;
+        const bool inside = r >= r_lo && r < r_hi && cc >= 0 && cc < nc;
+        // edges: bit 0 north, 1 south, 2 west, 3 east
+        const int kop = inside ? (cc == 0 && (edges & 4)) + (cc == nc - 1 && (edges & 8)) +
+                                     (r == 0 && (edges & 1)) + (r == nr - 1 && (edges & 2))
+                               : 0;
+        if (kop) {
+            int cap;
+            q[j] = open_q<float, MATH_EXACT>(get2(z, j), get2(h, j), get2(n, j), M_LAND, k, cap);
+            if (j == 0 ? own0 : own1)
+                o.cap += (unsigned)(cap * kop);
+            a[j] = open_sum<float>(q[j], kop);
+            o.ko |= (unsigned)((1 << kop) - 1) << (4 * j);
+        }
+    }
+    o.qo = mk2(q[0], q[1]);
+    o.add = mk2(a[0], a[1]);
+    return o;
+}
+
+// The registers of the four-row ring (see the file comment).
+template <int K>
+struct PairRing {
+    f2 z[4], h[4], n[4], L[4];          // row data, old level z + h
+    f2 zr[4], hr[4], nr[4], Lr[4];      // right-shifted copies (K = 8 SW faces)
+    f2 Xp[4], Xn[4];                    // x faces (c -> c+1) of a row, positive / negative part
+    f2 Yp[4], Yn[4];                    // y faces (r -> r+1), by the upper row
+    f2 Ep[4], En[4], Wp[4], Wn[4];      // K = 8: SE (r,c)->(r+1,c+1), SW (r,c+1)->(r+1,c)
+    f2 s[4];                            // limiter
+    f2 Qy[4], Qe[4], Qw[4];             // scaled y / SE / SW discharges, by the upper row
+    f2 hn[4], Ln[4], n6[4];             // new depth, new level (NaN outside the grid), n^6
+    f2 hm[4], cr[4];                    // hmax, rain field
+    f2 qo[4];                           // open-edge discharge of edge cells
+    unsigned ko[4];                     // open sides of the two cells (4 bits each)
+    unsigned ef[4];                     // stage-E candidates (bit per half)
+};
+
+// Per-segment values of the pair sweep.
+struct PairSeg {
+    const float *gz, *gn, *hin, *gcr;
+    float *hout, *ghmax, *gtmax;
+    long long pitch, colo;
+    int nr, nc, r0, r1, r_lo, r_hi;
+    int cbase, edges;                   // open edges: bit 0 N, 1 S, 2 W, 3 E (0: closed)
+    bool out_lane, edge_strip, col0ok, col1ok;
+    float thr, thr2c, T6;               // stage-E thresholds (warp-uniform)
+};
+
+template <typename AccT, int K, int MATH, bool RAINF>
+struct PairSweep {
+    using SS = StepSums<float, AccT>;
+
+    // thr = max(warp maximum so far, seed); thr2c = thr^2 (1 - 1e-6) for the
+    // critical-velocity prefilter; T6 = thr^6 (1 - 2e-4) for the bound (0 when
+    // thr < 1e-6: every velocity is at least 1e-6, physics.h:214-216)
+    static __device__ __forceinline__ void thresholds(PairSeg &G, float wmax, float vseed)
+    {
+        const float thr = wmax > vseed ? wmax : vseed;
+        G.thr = thr;
+        G.thr2c = thr * thr * 0.999999f;
+        const float t2 = thr * thr;
+        G.T6 = thr >= 1e-6f ? t2 * t2 * t2 * 0.9998f : 0.0f;
+    }
+
+    // one iteration of the pipeline; J = (i - i0) & 3
+    template <int J>
+    static __device__ __forceinline__ void iter(PairRing<K> &R, PairSeg &G, const PairK &c,
+                                                const StepVals<float> &sv, const RunK<float> &rk,
+                                                const StepK<float> *kp, SS &ss, int i)
+    {
+        constexpr int S1 = (J + 1) & 3;   // row i+1
+        constexpr int S0 = J & 3;         // row i
+        constexpr int Sm1 = (J + 3) & 3;  // row i-1
+        constexpr int Sm2 = (J + 2) & 3;  // row i-2
+        constexpr int Sm3 = (J + 1) & 3;  // row i-3
+        constexpr int Sm4 = J & 3;        // row i-4
+        const long long pitch = G.pitch;
+        const f2 z0 = bc2(0.0f);
+
+        // ---- loads: row i+1, and hmax / rain field of row i-1
+        {
+            const long long off = (long long)(i + 1 + PADR) * pitch + G.colo;
+            R.z[S1] = ld2(G.gz + off);
+            R.h[S1] = ld2(G.hin + off);
+            R.n[S1] = ld2(G.gn + off);
+            const int ra = min(i + 1 + PF_ROWS, G.nr + PADR - 1);
+            const long long offa = (long long)(ra + PADR) * pitch + G.colo;
+            prefetch_l2(G.gz + offa);
+            prefetch_l2(G.hin + offa);
+            prefetch_l2(G.gn + offa);
+            const long long off1 = off - 2 * pitch;
+            if (G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1)
+                R.hm[Sm1] = ld2_rw(G.ghmax + off1);
+            if constexpr (RAINF)
+                R.cr[Sm1] = ld2(G.gcr + off1);
+        }
+
+        // ---- A: x faces of row i; y (and diagonal) faces between rows i-1 and i
+        {
+            R.L[S0] = add2(R.z[S0], R.h[S0]);
+            const f2 zr = right2(R.z[S0]), Lr = right2(R.L[S0]), nrr = right2(R.n[S0]);
+            bool ux0, ux1, uy0, uy1;
+            f2 X = face2<MATH>(R.L[S0], Lr, R.z[S0], zr, R.n[S0], nrr, c.dx, c.rdx, c.w, c,
+                               ux0, ux1);
+            f2 Y = face2<MATH>(R.L[Sm1], R.L[S0], R.z[Sm1], R.z[S0], R.n[Sm1], R.n[S0], c.dx, c.rdx,
+                               c.w, c, uy0, uy1);
+            f2 E = z0, W = z0;
+            bool ue0 = false, ue1 = false, uw0 = false, uw1 = false;
+            if constexpr (K == 8) {
+                R.zr[S0] = zr;
+                R.Lr[S0] = Lr;
+                R.nr[S0] = nrr;
+                E = face2<MATH>(R.L[Sm1], Lr, R.z[Sm1], zr, R.n[Sm1], nrr, c.dd, c.rdd, c.w, c, ue0,
+                                ue1);
+                W = face2<MATH>(R.Lr[Sm1], R.L[S0], R.zr[Sm1], R.z[S0], R.nr[Sm1], R.n[S0], c.dd,
+                                c.rdd, c.w, c, uw0, uw1);
+            }
+            // faces are counted by the cell that holds them: x faces by row i,
+            // y and diagonal faces by row i-1
+            const bool ownA = G.out_lane && i >= G.r0 && i < G.r1;
+            const bool ownB = G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1;
+            if constexpr (MATH == MATH_EXACT) {
+                bool any = ux0 || ux1 || uy0 || uy1;
+                if constexpr (K == 8)
+                    any = any || ue0 || ue1 || uw0 || uw1;
+                const bool settle = __any_sync(0xffffffffu, any);
+                f2 hr = z0;
+                if (K == 8 || settle)
+                    hr = right2(R.h[S0]);
+                if constexpr (K == 8)
+                    R.hr[S0] = hr;
+                if (settle) {
+                    if (ux0 || ux1) {
+                        const Settled o = face2_settle(X, ux0, ux1, R.z[S0], R.h[S0], R.n[S0], zr,
+                                                       hr, nrr, false, kp);
+                        X = o.Q;
+                        if (ownA)
+                            ss.capn += o.cap;
+                    }
+                    if (uy0 || uy1) {
+                        const Settled o = face2_settle(Y, uy0, uy1, R.z[Sm1], R.h[Sm1], R.n[Sm1],
+                                                       R.z[S0], R.h[S0], R.n[S0], false, kp);
+                        Y = o.Q;
+                        if (ownB)
+                            ss.capn += o.cap;
+                    }
+                    if constexpr (K == 8) {
+                        if (ue0 || ue1) {
+                            const Settled o = face2_settle(E, ue0, ue1, R.z[Sm1], R.h[Sm1],
+                                                           R.n[Sm1], zr, hr, nrr, true, kp);
+                            E = o.Q;
+                            if (ownB)
+                                ss.capn += o.cap;
+                        }
+                        if (uw0 || uw1) {
+                            const Settled o = face2_settle(W, uw0, uw1, R.zr[Sm1], R.hr[Sm1],
+                                                           R.nr[Sm1], R.z[S0], R.h[S0], R.n[S0],
+                                                           true, kp);
+                            W = o.Q;
+                            if (ownB)
+                                ss.capn += o.cap;
+                        }
+                    }
+                }
+            } else {
+                if (ownA)
+                    ss.capn += (unsigned)ux0 + (unsigned)ux1;
+                if (ownB) {
+                    ss.capn += (unsigned)uy0 + (unsigned)uy1;
+                    if constexpr (K == 8)
+                        ss.capn += (unsigned)ue0 + (unsigned)ue1 + (unsigned)uw0 + (unsigned)uw1;
+                }
+            }
+            R.Xp[S0] = max2(X, z0);
+            R.Xn[S0] = min2(X, z0);
+            R.Yp[Sm1] = max2(Y, z0);
+            R.Yn[Sm1] = min2(Y, z0);
+            if constexpr (K == 8) {
+                R.Ep[Sm1] = max2(E, z0);
+                R.En[Sm1] = min2(E, z0);
+                R.Wp[Sm1] = max2(W, z0);
+                R.Wn[Sm1] = min2(W, z0);
+            }
+        }
+
+        // ---- C: outflow volume and limiter of row i-1 (model.c:180-238,
+        //      489-502), in the reference order +x, -x, +y, -y, d1+, d1-,
+        //      d2+, d2-, open slots
+        {
+            const int r = i - 1;
+            f2 out = sub2(R.Xp[Sm1], left2(R.Xn[Sm1]));
+            out = add2(out, R.Yp[Sm1]);
+            out = sub2(out, R.Yn[Sm2]);
+            if constexpr (K == 8) {
+                out = add2(out, R.Ep[Sm1]);
+                out = sub2(out, left2(R.En[Sm2]));
+                out = add2(out, left2(R.Wp[Sm1]));
+                out = sub2(out, R.Wn[Sm2]);
+            }
+            R.ko[Sm1] = 0u;
+            if (G.edges) {
+                const bool erow = (r == 0 && (G.edges & 1)) || (r == G.nr - 1 && (G.edges & 2));
+                if (erow || G.edge_strip) {
+                    const bool own = G.out_lane && r >= G.r0 && r < G.r1;
+                    const OpenFaces o = open_faces2(R.z[Sm1], R.h[Sm1], R.n[Sm1], r, G.cbase,
+                                                    G.nr, G.nc, G.r_lo, G.r_hi, G.edges,
+                                                    own && G.col0ok, own && G.col1ok, kp);
+                    R.ko[Sm1] = o.ko;
+                    R.qo[Sm1] = o.qo;
+                    ss.capn += o.cap;
+                    out = add2(out, o.add);
+                }
+            }
+            const f2 ov = mul2(out, c.dt);
+            const f2 hold = mul2(R.h[Sm1], c.A);
+            const f2 hz = max2(hold, z0);
+            const bool l0 = lo2(ov) > lo2(hz), l1 = hi2(ov) > hi2(hz);
+            R.s[Sm1] = bc2(1.0f);
+            if (__any_sync(0xffffffffu, l0 || l1)) {
+                const f2 o = sel2(l0, l1, ov, bc2(1.0f));
+                f2 q;
+                if constexpr (MATH == MATH_EXACT)
+                    q = div2_mk(hold, o, rcp2_nr(o));
+                else
+                    q = mul2(hold, rcp_2(o));
+                R.s[Sm1] = sel2(l0, l1, q, bc2(1.0f));
+            }
+        }
+
+        // ---- D: scaled discharges of the faces below and right of row i-2,
+        //      net inflow, depth update, clamp, inflow, hmax/tmax, stage-E
+        //      candidates (model.c:511-597)
+        {
+            const int r = i - 2;
+            const bool row_out = r >= G.r0 && r < G.r1;
+            const f2 s0 = R.s[Sm2];
+            const f2 sr = right2(s0);
+            const f2 Qsx = fma2(R.Xn[Sm2], sr, mul2(R.Xp[Sm2], s0));
+            const f2 Qsy = fma2(R.Yn[Sm2], R.s[Sm1], mul2(R.Yp[Sm2], s0));
+            R.Qy[Sm2] = Qsy;
+            f2 net = sub2(z0, Qsx);
+            net = add2(net, left2(Qsx));
+            net = sub2(net, Qsy);
+            net = add2(net, R.Qy[Sm3]);
+            if constexpr (K == 8) {
+                const f2 Qse = fma2(R.En[Sm2], right2(R.s[Sm1]), mul2(R.Ep[Sm2], s0));
+                const f2 Qsw = fma2(R.Wn[Sm2], R.s[Sm1], mul2(R.Wp[Sm2], sr));
+                R.Qe[Sm2] = Qse;
+                R.Qw[Sm2] = Qsw;
+                net = sub2(net, Qse);
+                net = add2(net, left2(R.Qe[Sm3]));
+                net = sub2(net, left2(Qsw));
+                net = add2(net, R.Qw[Sm3]);
+            }
+            const bool cell0 = row_out && G.out_lane && G.col0ok;
+            const bool cell1 = row_out && G.out_lane && G.col1ok;
+            if (G.edges && __any_sync(0xffffffffu, R.ko[Sm2] != 0u)) {
+                // open-edge outflow scaled by the cell's own limiter
+                // (model.c:553-559), summed over its open slots
+                float qb[2];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const unsigned kk = (R.ko[Sm2] >> (4 * j)) & 15u;
+                    qb[j] = open_sum<float>(get2(R.qo[Sm2], j) * get2(s0, j), __popc(kk));
+                }
+                net = sub2(net, mk2(qb[0], qb[1]));
+                if (cell0 && (R.ko[Sm2] & 15u))
+                    ss.a_bnd += acc_mul<AccT, float>(sv.dt, qb[0]);
+                if (cell1 && (R.ko[Sm2] >> 4))
+                    ss.a_bnd += acc_mul<AccT, float>(sv.dt, qb[1]);
+            }
+            f2 rain = c.rain;
+            if constexpr (RAINF)
+                rain = mul2(R.cr[Sm2], bc2(sv.F));
+            f2 dq;
+            if constexpr (MATH == MATH_EXACT)
+                dq = div2_mk(net, c.A, c.invA);
+            else
+                dq = mul2(net, c.invA);
+            f2 hu = add2(R.h[Sm2], add2(mul2(c.dt, dq), rain));
+            {
+                float u0, u1;
+                sp2(hu, u0, u1);
+                if (__any_sync(0xffffffffu, u0 < 0.0f || u1 < 0.0f)) {
+                    if (u0 < 0.0f) {
+                        if (cell0)
+                            ss.a_clamp += acc_mul<AccT, float>(-u0, sv.A);
+                        u0 = 0.0f;
+                    }
+                    if (u1 < 0.0f) {
+                        if (cell1)
+                            ss.a_clamp += acc_mul<AccT, float>(-u1, sv.A);
+                        u1 = 0.0f;
+                    }
+                    hu = mk2(u0, u1);
+                }
+            }
+            if (r == rk.inflow_r) {
+                const int d = rk.inflow_c - G.cbase;
+                if (d == 0)
+                    hu = mk2(lo2(hu) + sv.inflow_dh, hi2(hu));
+                else if (d == 1)
+                    hu = mk2(lo2(hu), hi2(hu) + sv.inflow_dh);
+            }
+            if constexpr (sizeof(AccT) == 4) {
+                if (cell0)
+                    ss.a_rain += sv.A * lo2(rain);
+                if (cell1)
+                    ss.a_rain += sv.A * hi2(rain);
+            } else if constexpr (RAINF) {
+                ss.rain_sum += (cell0 ? (double)lo2(rain) : 0.0) + (cell1 ? (double)hi2(rain) : 0.0);
+            }
+            // new level for stage E (NaN outside the grid: no neighbour
+            // there); cells outside the grid keep their padding depth
+            f2 Ln = add2(R.z[Sm2], hu);
+            f2 hkeep = hu;
+            if (G.edge_strip || r < G.r_lo || r >= G.r_hi) {
+                const bool rin = r >= G.r_lo && r < G.r_hi;
+                const bool in0 = rin && G.col0ok, in1 = rin && G.col1ok;
+                Ln = sel2(in0, in1, Ln, bc2(__int_as_float(0x7fc00000)));
+                hkeep = sel2(in0, in1, hu, R.h[Sm2]);
+            }
+            R.Ln[Sm2] = Ln;
+            R.hn[Sm2] = hu;
+            // stage-E candidates: wet output cells whose critical velocity
+            // sqrt(g h) may exceed the warp's threshold (margin 1e-6)
+            unsigned ef = 0u;
+            if (sv.want_v) {
+                const f2 gh = mul2(c.g, hu);
+                const bool t = G.thr > 0.0f;
+                if (cell0 && lo2(hu) >= c.tau_h && !(t && lo2(gh) <= G.thr2c))
+                    ef |= 1u;
+                if (cell1 && hi2(hu) >= c.tau_h && !(t && hi2(gh) <= G.thr2c))
+                    ef |= 2u;
+                const f2 n2 = mul2(R.n[Sm2], R.n[Sm2]);
+                R.n6[Sm2] = mul2(mul2(n2, n2), n2);
+            }
+            R.ef[Sm2] = ef;
+            // hmax / tmax of output cells
+            const f2 hmo = R.hm[Sm2];
+            const bool rise0 = cell0 && lo2(hu) > lo2(hmo);
+            const bool rise1 = cell1 && hi2(hu) > hi2(hmo);
+            if (row_out && G.out_lane) {
+                const long long off2 = (long long)(r + PADR) * pitch + G.colo;
+                st2(G.hout + off2, hkeep);
+                if (rise0 || rise1) {
+                    st2(G.ghmax + off2, sel2(rise0, rise1, hu, hmo));
+                    if (rise0)
+                        G.gtmax[off2] = sv.tmax_val;
+                    if (rise1)
+                        G.gtmax[off2 + 1] = sv.tmax_val;
+                }
+            }
+        }
+
+        // ---- E: next step's stable velocity of row i-3 from the new levels
+        //      of rows i-4..i-2 (physics.h:158-217), for the candidates
+        if (sv.want_v && __any_sync(0xffffffffu, R.ef[Sm3] != 0u)) {
+            const int r = i - 3;
+            const f2 la = R.Ln[Sm3];
+            f2 mo = max2(abs2(sub2(la, right2(la))), abs2(sub2(la, left2(la))));
+            mo = max2(mo, max2(abs2(sub2(la, R.Ln[Sm2])), abs2(sub2(la, R.Ln[Sm4]))));
+            mo = max2(mo, z0);
+            f2 md = z0;
+            if constexpr (K == 8) {
+                const f2 lb = R.Ln[Sm2], lt = R.Ln[Sm4];
+                md = max2(abs2(sub2(la, right2(lb))), abs2(sub2(la, left2(lb))));
+                md = max2(md, max2(abs2(sub2(la, right2(lt))), abs2(sub2(la, left2(lt)))));
+                md = max2(md, z0);
+            }
+            if (G.edges) {
+                const bool erow = (r == 0 && (G.edges & 1)) || (r == G.nr - 1 && (G.edges & 2));
+                if (erow || G.edge_strip) {
+                    // the open virtual neighbour z - S_bnd*dx, h = 0 (physics.h:183-189)
+                    const long long off3 = (long long)(r + PADR) * pitch + G.colo;
+                    const f2 z3 = ld2(G.gz + off3);
+                    const f2 dv = abs2(sub2(la, sub2(z3, bc2(sv.k.S_bnd * sv.k.dx))));
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        const int cc = G.cbase + j;
+                        if (erow || (cc == 0 && (G.edges & 4)) || (cc == G.nc - 1 && (G.edges & 8)))
+                            put2(mo, j, fmaxf(get2(mo, j), get2(dv, j)));
+                    }
+                }
+            }
+            // bound: v^6 <= h^4 S^3 / n^6 (S = the largest slope), against thr^6
+            f2 S = mul2(mo, c.rdx);
+            if constexpr (K == 8)
+                S = max2(S, mul2(md, c.rdd));
+            const f2 hv = R.hn[Sm3];
+            const f2 h2 = mul2(hv, hv);
+            const f2 lhs = mul2(mul2(h2, h2), mul2(mul2(S, S), S));
+            const f2 rhs = mul2(R.n6[Sm3], bc2(G.T6));
+            const unsigned ef = R.ef[Sm3];
+            const bool x0 = (ef & 1u) && (lo2(lhs) >= lo2(rhs) || lo2(lhs) < 1e-30f);
+            const bool x1 = (ef & 2u) && (hi2(lhs) >= hi2(rhs) || hi2(lhs) < 1e-30f);
+            if (__any_sync(0xffffffffu, x0 || x1)) {
+                const long long off3 = (long long)(r + PADR) * pitch + G.colo;
+                const f2 n3 = ld2(G.gn + off3);
+                float vm = ss.vmax;
+                if (x0 || x1)
+                    vm = pair_velocity<K, MATH>(vm, x0, x1, mo, md, hv, n3, kp);
+                ss.vmax = vm;
+                thresholds(G, warp_max_nonneg(vm), sv.vseed);
+            }
+        }
+    }
+
+    // One warp streams output rows [r0, r1) of one strip (as sweep_segment).
+    // kp: the step constants in shared memory, for the exact re-evaluations.
+    static __device__ void run(const GridD<float> &g, const RunK<float> &rk,
+                               const StepVals<float> &sv, const StepK<float> *kp, int strip, int r0,
+                               int r1, int lane, SS &ss)
+    {
+        using Gm = Geom<2>;
+        PairSeg G;
+        G.gz = g.z;
+        G.gn = g.n;
+        G.gcr = g.cr;
+        G.hin = sv.hin;
+        G.hout = sv.hout;
+        G.ghmax = g.hmax;
+        G.gtmax = g.tmax;
+        G.pitch = g.pitch;
+        G.nr = g.nr;
+        G.nc = g.nc;
+        G.r0 = r0;
+        G.r1 = r1;
+        G.r_lo = g.r_lo;
+        G.r_hi = g.r_hi;
+        G.cbase = strip * Gm::OW - Gm::HL + lane * 2;
+        G.colo = (long long)(G.cbase + PADC);
+        G.out_lane = lane * 2 >= Gm::HL && lane * 2 < Gm::HL + Gm::OW;
+        G.col0ok = G.cbase >= 0 && G.cbase < g.nc;
+        G.col1ok = G.cbase + 1 >= 0 && G.cbase + 1 < g.nc;
+        G.edges = rk.open ? (rk.edge_n ? 1 : 0) | (rk.edge_s ? 2 : 0) | (rk.edge_w ? 4 : 0) |
+                                (rk.edge_e ? 8 : 0)
+                          : 0;
+        // strips that hold a column outside the grid or column 0 / nc-1
+        const int c_first = strip * Gm::OW - Gm::HL;
+        G.edge_strip = c_first <= 0 || c_first + Gm::SW > g.nc - 1;
+        thresholds(G, sv.want_v ? warp_max_nonneg(ss.vmax) : 0.0f, sv.vseed);
+
+        const StepK<float> &k = sv.k;
+        PairK c;
+        c.dx = bc2(k.dx);
+        c.rdx = bc2(k.rdx);
+        c.dd = bc2(k.d_diag);
+        c.rdd = bc2(k.rdd);
+        c.w = bc2(k.w);
+        c.A = bc2(k.A);
+        c.invA = bc2(k.inv_A);
+        c.g = bc2(k.g);
+        c.dt = bc2(sv.dt);
+        c.rain = bc2(sv.rainv);
+        c.half = bc2(0.5f);
+        c.nmin = bc2(1e-12f);
+        c.vcrK = bc2(0.99999905f);
+        // exact mode: below A/(2K dt) by more than the roundings of the
+        // estimate, so a face whose |dL| * capK exceeds Qm is surely not
+        // capped; fast mode: RN(1/(2K dt)), the cap being (|dL| A) capK
+        c.capK = MATH == MATH_EXACT ? bc2(k.A * k.rden * 0.99999809f) : bc2(k.rden);
+        c.tau_l = k.tau_l;
+        c.tau_h = k.tau_h;
+
+        // iterations i0 .. r1+2, a multiple of four; the extra leading
+        // iterations compute rows above the segment's halo only
+        const int n_it = ((r1 - r0 + 6) + 3) & ~3;
+        const int i0 = r1 + 3 - n_it;
+
+        PairRing<K> R;
+        const f2 z0 = bc2(0.0f);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            R.z[q] = R.h[q] = R.n[q] = R.L[q] = z0;
+            R.zr[q] = R.hr[q] = R.nr[q] = R.Lr[q] = z0;
+            R.Xp[q] = R.Xn[q] = R.Yp[q] = R.Yn[q] = z0;
+            R.Ep[q] = R.En[q] = R.Wp[q] = R.Wn[q] = z0;
+            R.s[q] = bc2(1.0f);
+            R.Qy[q] = R.Qe[q] = R.Qw[q] = z0;
+            R.hn[q] = R.n6[q] = R.hm[q] = R.cr[q] = R.qo[q] = z0;
+            R.Ln[q] = bc2(__int_as_float(0x7fc00000));
+            R.ko[q] = R.ef[q] = 0u;
+        }
+        {
+            const long long off = (long long)(i0 + PADR) * G.pitch + G.colo;
+            R.z[0] = ld2(G.gz + off);
+            R.h[0] = ld2(G.hin + off);
+            R.n[0] = ld2(G.gn + off);
+        }
+        for (int i = i0; i < i0 + n_it; i += 4) {
+            iter<0>(R, G, c, sv, rk, kp, ss, i);
+            iter<1>(R, G, c, sv, rk, kp, ss, i + 1);
+            iter<2>(R, G, c, sv, rk, kp, ss, i + 2);
+            iter<3>(R, G, c, sv, rk, kp, ss, i + 3);
+        }
+        // uniform rain on LAND output cells, counted per lane
+        if constexpr (sizeof(AccT) == 8 && !RAINF) {
+            if (G.out_lane)
+                ss.rain_cells += (long long)(r1 - r0) * ((G.col0ok ? 1 : 0) + (G.col1ok ? 1 : 0));
+        }
+    }
+};
+
+}  // namespace fcab

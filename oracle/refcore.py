@@ -53,6 +53,9 @@ def build(ref_root: str = "/root/reference") -> bool:
     if (ROOT / "floodca_b200" / "libfloodca_b200.so").exists():
         subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}",
                         "dropin"], check=True)
+    # the same CLI on the reference's own CUDA backend (same-box GPU comparison)
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile.ref"), f"REF={ref_root}",
+                    "refcuda"], check=True)
     return True
 
 

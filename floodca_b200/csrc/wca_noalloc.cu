@@ -31,8 +31,8 @@ using namespace fcab;
 
 namespace {
 
-// Capacity in padded cells: (nrows + 8) * round_up(ncols + 132, 32) must not
-// exceed it (a 512 x 768 grid fits, as does any grid of up to ~400k cells).
+// Capacity in padded cells: (nrows + 16) * round_up(ncols + 132, 32) must not
+// exceed it (a 512 x 768 grid fits, as does any grid of up to ~390k cells).
 constexpr long long NOALLOC_MAX_PADDED = 1ll << 19;
 constexpr size_t CTL_BYTES = (sizeof(Ctl) + 255) / 256 * 256;
 constexpr size_t FIELD_BYTES = (size_t)NOALLOC_MAX_PADDED * sizeof(float);
@@ -113,13 +113,36 @@ __global__ void k_unpack(GridD<float> g, const Ctl *ctl, float *h, float *hmax, 
     }
 }
 
-__global__ void k_ctl_start(Ctl *c)
+// Starts the control block; the inflow cell is checked here, on the device
+// (a cell that is not LAND receives no inflow volume), so the call never
+// waits for the stream.
+__global__ void k_ctl_start(Ctl *c, const uint8_t *mask, long long inflow_cell)
 {
     c->t = 0.0;
     c->step = 0;
     c->dt_base = 0.0;
     c->force_day = -1;
     c->h_cur = 0;
+    c->inflow_off = inflow_cell >= 0 && mask[inflow_cell] != M_LAND;
+}
+
+// Open faces per step: one per LAND cell on each open edge
+// (FloodCA src/common/model.c:442-479), summed into *count.
+__global__ void k_count_open(const uint8_t *mask, int nr, int nc, int en, int es, int ew, int ee,
+                             unsigned long long *count)
+{
+    unsigned long long n = 0;
+    const long long N = (long long)nr * nc;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (mask[i] != M_LAND)
+            continue;
+        const int r = (int)(i / nc), c = (int)(i % nc);
+        n += (r == 0 && en) + (r == nr - 1 && es) + (c == 0 && ew) + (c == nc - 1 && ee);
+    }
+    n = warp_sum(n);
+    if ((threadIdx.x & 31) == 0 && n)
+        atomicAdd(count, n);
 }
 
 }  // namespace
@@ -131,8 +154,8 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
 {
     if (!cfg || !z || !n || !mask || !h || !hmax)
         return noalloc_fail(FCAB_ERR_ARG, "cfg, z, n, mask, h and hmax are required");
-    if (h == hmax)
-        return noalloc_fail(FCAB_ERR_ARG, "h and hmax must be distinct arrays");
+    if (h == hmax || (tmax && (tmax == h || tmax == hmax)))
+        return noalloc_fail(FCAB_ERR_ARG, "h, hmax and tmax must be distinct arrays");
     if (cfg->precision != FCAB_PREC_F32)
         return noalloc_fail(FCAB_ERR_ARG, "only the FP32 precision (FCAB_PREC_F32) is available");
     if (cfg->max_steps <= 0)
@@ -161,8 +184,10 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     float *fz = f, *fn = f + nelem, *fh0 = f + 2 * nelem, *fh1 = f + 3 * nelem;
     float *fhm = f + 4 * nelem, *ftm = f + 5 * nelem, *fcr = f + 6 * nelem;
     uint8_t *fm = reinterpret_cast<uint8_t *>(f + 7 * nelem);
+    // misc: V0, V, open faces per step
     double *vol = reinterpret_cast<double *>(base + CTL_BYTES + 7 * FIELD_BYTES +
                                              NOALLOC_MAX_PADDED);
+    unsigned long long *nopen = reinterpret_cast<unsigned long long *>(vol + 2);
     g.z = fz;
     g.n = fn;
     g.cr = fcr;
@@ -188,28 +213,31 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     NA_TRY(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
     NA_TRY(cudaMemsetAsync(f, 0, 7 * (size_t)nelem * sizeof(float), s));
     NA_TRY(cudaMemsetAsync(fm, M_WALL, (size_t)nelem, s));
+    NA_TRY(cudaMemsetAsync(vol, 0, 256, s));
     PackDst pd{fz, fn, fh0, fhm, ftm, fcr, fm, pitch, cfg->nrows, cfg->ncols};
     k_pack<<<512, 256, 0, s>>>(z, n, C, Rday, mask, h, hmax, tmax, pd);
     NA_TRY(cudaGetLastError());
-    k_ctl_start<<<1, 1, 0, s>>>(ctl);
+    const bool inflow_set =
+        cfg->inflow_cell >= 0 && cfg->inflow_cell < (long long)cfg->nrows * cfg->ncols;
+    k_ctl_start<<<1, 1, 0, s>>>(ctl, mask, inflow_set ? cfg->inflow_cell : -1);
     NA_TRY(cudaGetLastError());
+    if (stats && cfg->boundary == FCA_BND_OPEN) {
+        k_count_open<<<128, 256, 0, s>>>(mask, cfg->nrows, cfg->ncols, cfg->edge_n, cfg->edge_s,
+                                         cfg->edge_w, cfg->edge_e, nopen);
+        NA_TRY(cudaGetLastError());
+    }
 
     RunK<float> rk;
     TimeCfg tc;
     make_run_params_f32(*cfg, &rk, &tc);
     rk.has_sea = 1;          // the generic kernel tests SEA neighbours itself
     rk.cr_uniform = 0.0f;
-    if (cfg->inflow_cell >= 0 && cfg->inflow_cell < (long long)cfg->nrows * cfg->ncols) {
-        uint8_t mi = M_WALL;
-        NA_TRY(cudaMemcpyAsync(&mi, mask + cfg->inflow_cell, 1, cudaMemcpyDeviceToHost, s));
-        NA_TRY(cudaStreamSynchronize(s));
-        tc.inflow_ok = mi == M_LAND;
-    }
+    tc.inflow_ok = inflow_set ? 1 : 0;      // k_ctl_start drops it for a non-LAND cell
 
     VariantKey key;
     key.prec = FCAB_PREC_F32;
     key.K = cfg->K;
-    key.cpl = cfg->ncols <= 64 ? 1 : 2;
+    key.cpl = pick_cpl(*cfg);
     key.math = cfg->math == FCAB_MATH_FAST ? MATH_FAST : MATH_EXACT;
     key.rainf = 1;
     key.landonly = 0;
@@ -221,16 +249,9 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     NA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     NA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.step_fn, L.threads, 0));
     const int wpb = L.threads / 32;
-    const int ow = 32 * key.cpl - 2 * (key.cpl == 1 ? 3 : 4);
-    const long long total = ((cfg->ncols + ow - 1) / ow) * (long long)cfg->nrows;
-    long long warps = (total + 47) / 48;
-    const long long maxw = (long long)nsm * (per_sm > 0 ? per_sm : 1) * wpb;
-    warps = warps < maxw ? warps : maxw;
-    warps = warps < 1 ? 1 : warps;
-    const int grid = (int)((warps + wpb - 1) / wpb);
+    const int grid = (int)((step_warps(*cfg, key.cpl, nsm, per_sm, wpb) + wpb - 1) / wpb);
 
     if (stats) {   // V0, the LAND volume of the initial depth
-        NA_TRY(cudaMemsetAsync(vol, 0, 2 * sizeof(double), s));
         k_volume<float><<<256, 256, 0, s>>>(g, ctl, rk.k.A, vol);
         NA_TRY(cudaGetLastError());
     }
@@ -245,8 +266,10 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
         NA_TRY(cudaGetLastError());
         Ctl hc;
         double V[2] = {0.0, 0.0};
+        unsigned long long nop = 0;
         NA_TRY(cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
         NA_TRY(cudaMemcpyAsync(V, vol, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NA_TRY(cudaMemcpyAsync(&nop, nopen, sizeof(nop), cudaMemcpyDeviceToHost, s));
         NA_TRY(cudaStreamSynchronize(s));
         memset(stats, 0, sizeof(*stats));
         stats->t = hc.t;
@@ -264,6 +287,12 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
         }
         stats->V_in = hc.V_in;
         stats->dt_min_hits = hc.dt_min_hits;
+        stats->dt_full_passes = hc.full_passes;
+        // every face counts once per step (src/common/model.c:394-487)
+        const long long nr = cfg->nrows, nc = cfg->ncols;
+        const long long faces = nr * (nc - 1) + (nr - 1) * nc +
+                                (cfg->K == 8 ? 2 * (nr - 1) * (nc - 1) : 0) + (long long)nop;
+        stats->cap_total = faces * (long long)hc.step;
         double den = stats->V_rain + stats->V_in + stats->V0;
         den = den < 1e-30 ? 1e-30 : den;
         const double num = stats->V + stats->V_sea + stats->V_bnd - stats->V_rain -

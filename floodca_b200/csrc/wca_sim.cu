@@ -195,7 +195,7 @@ static void fill_runk(RunK<T> &rk, const FcabConfig &c, int hn = 0, int hs = 0)
     }
 }
 
-static int pick_cpl(const FcabConfig &c)
+int fcab::pick_cpl(const FcabConfig &c)
 {
     if (c.cols_per_lane == 1 || c.cols_per_lane == 2 || c.cols_per_lane == 4)
         return c.cols_per_lane;
@@ -206,6 +206,22 @@ static int pick_cpl(const FcabConfig &c)
     if (c.ncols <= 64 || strips2 * c.nrows < 40960)
         return 1;
     return 2;
+}
+
+long long fcab::step_warps(const FcabConfig &c, int cpl, int nsm, int per_sm, int wpb)
+{
+    const int ow = 32 * cpl - 2 * (cpl == 1 ? 3 : 4);
+    const long long strips = (c.ncols + ow - 1) / ow;
+    const long long total = strips * c.nrows;
+    const long long max_warps = (long long)nsm * (per_sm > 0 ? per_sm : 1) * wpb;
+    // rows per warp: enough warps to fill the resident slots, but at least 4
+    // rows per warp (each warp's segment costs 6 extra pipeline rows)
+    long long seg = c.seg_rows > 0 ? c.seg_rows : total / max_warps;
+    if (seg < 4)
+        seg = 4;
+    const long long want = (total + seg - 1) / seg;
+    const long long warps = want < max_warps ? want : max_warps;
+    return warps < 1 ? 1 : warps;
 }
 
 extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *stream)
@@ -538,21 +554,8 @@ static int resolve_variant(FcabSim *s)
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->L.step_fn, s->L.threads, 0));
     if (per_sm < 1)
         per_sm = 1;
-    const int ow = 32 * s->cpl - 2 * (s->cpl == 1 ? 3 : 4);
-    const long long strips = (s->cfg.ncols + ow - 1) / ow;
-    const long long total = strips * s->cfg.nrows;
     const int wpb = s->L.threads / 32;     // warps per CTA
-    long long max_warps = (long long)nsm * per_sm * wpb;
-    // rows per warp: enough warps to fill the resident slots, but at least 4
-    // rows per warp (each warp's segment costs 6 extra pipeline rows)
-    long long seg = s->cfg.seg_rows > 0 ? s->cfg.seg_rows : total / max_warps;
-    if (seg < 4)
-        seg = 4;
-    long long want_warps = (total + seg - 1) / seg;
-    long long warps = want_warps < max_warps ? want_warps : max_warps;
-    if (warps < 1)
-        warps = 1;
-    s->grid = (int)((warps + wpb - 1) / wpb);
+    s->grid = (int)((step_warps(s->cfg, s->cpl, nsm, per_sm, wpb) + wpb - 1) / wpb);
     s->warps_total = s->grid * wpb;
     s->occupancy = per_sm;
     if (s->graph) {

@@ -46,6 +46,13 @@ struct FcabSim {
 namespace fcab {
 // Records the calling thread's fcab_last_error() message (wca_sim.cu).
 void set_error(const char *msg);
+// Columns per lane of the step kernel for a configuration: cfg.cols_per_lane
+// when set (1, 2 or 4), else by grid size (wca_sim.cu).
+int pick_cpl(const FcabConfig &c);
+// Warps of the step kernel's grid: enough to fill the resident slots (nsm SMs,
+// per_sm CTAs of wpb warps) with segments of cfg.seg_rows rows when set,
+// else an even split, at least 4 rows per warp (wca_sim.cu).
+long long step_warps(const FcabConfig &c, int cpl, int nsm, int per_sm, int wpb);
 // Run constants of an FP32 configuration (defined in wca_sim.cu).
 void make_run_params_f32(const FcabConfig &cfg, RunK<float> *rk, TimeCfg *tc);
 // Row-block copies between dense pageable host rows and pitched device rows

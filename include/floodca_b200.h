@@ -373,16 +373,20 @@ FCAB_API void fcab_batch_destroy(FcabBatch *b);
  * running, since cudaMalloc/cudaFree synchronise the device and stall other
  * streams. The working memory is one library-global device array of 2^19
  * padded cells (about 15 MB, held on every GPU that loads the library until
- * exit): (nrows + 8) * round_up(ncols + 132, 32) must not exceed 524288
+ * exit): (nrows + 16) * round_up(ncols + 132, 32) must not exceed 524288
  * (e.g. 512 x 768), else FCAB_ERR_ARG. Inputs z, n, mask (row-major
  * nrows*ncols, device), optional C and Rday (NULL: no rain); h and hmax are
  * read as the initial state and overwritten with the final state, tmax too
- * (NULL: start at 0, not written back). stream: cudaStream_t, NULL for the
- * legacy stream. stats (host, may be NULL) receives the run totals after a
- * stream synchronisation. The first call on each device looks up the array's
- * device address; make that first call before any stream capture. Calls
- * share the array: calls that overlap on the GPU (other streams, other host
- * threads) race and corrupt each other. */
+ * (NULL: start at 0, not written back); h, hmax and tmax must be distinct.
+ * cfg->cols_per_lane and cfg->seg_rows set the launch shape as for sessions.
+ * An inflow cell that is not LAND receives nothing (checked on the device).
+ * stream: cudaStream_t, NULL for the legacy stream; without stats the call
+ * only enqueues work on it and returns. stats (host, may be NULL) receives
+ * the run totals after a stream synchronisation, cap_total and
+ * dt_full_passes included. The first call on each device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU (other streams, other
+ * host threads) race and corrupt each other. */
 FCAB_API int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const float *n,
                               const float *C, const float *Rday, const uint8_t *mask, float *h,
                               float *hmax, float *tmax, void *stream, FcabStats *stats);

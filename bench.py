@@ -40,7 +40,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Gcell-updates/s"
-BYTES_PER_CELL = 25  # read z, h, n, hmax (4 B each) + mask (1 B); write h, hmax (4 B each)
+# algorithmic bytes per cell-update: read z, h, n, hmax (4 B each), write h,
+# hmax (4 B each); the generic layout also reads the mask (1 B), the all-LAND
+# layout does not
+BYTES_LAND_ONLY, BYTES_GENERIC = 24, 25
 
 
 def warm_domain(n: int):
@@ -184,6 +187,44 @@ def e2e_mass_error(r: dict) -> float:
 
 
 # ---------------------------------------------------------------------------
+# The ensemble half of the metric: a seeded config-4 subset batched against
+# the same members one at a time through the same kernel.
+
+ENSEMBLE_MEMBERS = 32
+
+
+def ensemble_leg(math: str = "exact") -> dict:
+    from floodca_b200 import ensemble as E
+    allm = E.config4_members(256)
+    members = allm[::len(allm) // ENSEMBLE_MEMBERS]
+    tune = E.DEFAULT_TUNING
+    try:
+        table = json.loads(E.TUNING_FILE.read_text())
+        tune = table.get(E._tuning_key(math), tune)
+    except (OSError, ValueError):
+        pass
+    bat = E.run_batched(members, math, tune, window=0.0)
+    one = E.run_one_at_a_time(members, math)
+    same = all(a["step"] == b["step"] and a["t"] == b["t"]
+               for a, b in zip(bat["stats"], one["stats"]))
+    return {"workload": f"config 4 subset: {len(members)} members (every "
+                        f"{len(allm) // len(members)}th of the seeded 256), side "
+                        f"{min(m.side for m in members)}..{max(m.side for m in members)}, "
+                        "8 h simulated, 20-150 mm/h for 0.5-4 h, own terrain and n scale each",
+            "members": len(members),
+            "batched_members_per_hour": bat["members_per_hour"],
+            "one_at_a_time_members_per_hour": one["members_per_hour"],
+            "multiple": bat["members_per_hour"] / one["members_per_hour"],
+            "batched_wall_s": bat["wall_s"], "one_at_a_time_wall_s": one["wall_s"],
+            "batched_gcell_steps_per_s": bat["cell_steps"] / bat["wall_s"] / 1e9,
+            "one_at_a_time_gcell_steps_per_s": one["cell_steps"] / one["wall_s"] / 1e9,
+            "members_steps_and_times_equal": same,
+            "tuning": {k: tune[k] for k in ("cols_per_lane", "seg_rows_by_class")},
+            "timing": "host wall around the runs with device synchronisation; terrain "
+                      "generation and upload excluded (both arms)"}
+
+
+# ---------------------------------------------------------------------------
 # Per-configuration table: the same workloads on the GPU (sessions) and on the
 # reference's OpenMP core with all host threads and with one.
 
@@ -288,6 +329,7 @@ def main() -> int:
                     help="seconds of CPU time for the reference baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--config-table", action="store_true",
                     help="GPU vs reference CPU (all threads, one thread) on configs 1-3")
     ap.add_argument("--cpu-worker", nargs=2, metavar=("CONFIG", "STEPS"), help=argparse.SUPPRESS)
@@ -325,19 +367,20 @@ def main() -> int:
     info = sess.info()
     land = info["land_cells"]
     stream = torch.cuda.ExternalStream(sess.stream())
+    # clocks are sampled from the warm-up to the end of the last GPU leg
+    clk = ClockSampler(local).__enter__()
     sess.advance(args.warmup)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     l0 = sess.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        e0.record(stream)
-        sess.advance(args.steps)
-        e1.record(stream)
-        e1.synchronize()
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sess.advance(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
     launches = sess.launches() - l0
     ms = e0.elapsed_time(e1)
     st = sess.stats()
@@ -351,20 +394,22 @@ def main() -> int:
 
     value = world * land * args.steps / (ms / 1e3) / 1e9
     per_launch_s = ms / 1e3 / args.steps
-    alg_bytes = BYTES_PER_CELL * land
+    bytes_per_cell = BYTES_LAND_ONLY if info["land_only"] else BYTES_GENERIC
+    alg_bytes = bytes_per_cell * land
     peaks = measured_peaks()
     peak = peaks.get("hbm_gbs")
     achieved = alg_bytes / per_launch_s / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak or 6650.0, "unit": "GB/s",
             "frac": achieved / (peak or 6650.0), "traffic": profile_traffic(),
             "peak_source": "measured" if peak else "fallback",
-            "bytes_per_cell": BYTES_PER_CELL, "kernel": "k_step"}
+            "bytes_per_cell": bytes_per_cell, "kernel": "k_step",
+            "time": "CUDA events around the timed steps on the session stream"}
 
     out = {"metric": METRIC, "value": value, "unit": "Gcell/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic", "config": config_block(n, world), "roofline": roof,
-           "clocks": clk.summary(), "gpu_launches": int(launches),
+           "gpu_launches": int(launches),
            "all_steps_active": bool(active), "launch": info, "math": args.math}
 
     if not args.no_e2e:
@@ -401,8 +446,14 @@ def main() -> int:
                       "wall_s_each": walls, "statistic": "median", "rc": rc,
                       "E_mass": e2e_mass_error(res),
                       "t_h2d_s": g.tm.t_h2d, "t_d2h_s": g.tm.t_d2h}
+    if not args.no_ensemble:
+        out["ensemble"] = ensemble_leg(args.math)
+    clk.__exit__(None, None, None)
+    out["clocks"] = clk.summary()
+    out["clocks"]["span"] = "warm-up, timed steps, end-to-end and ensemble legs"
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = reference_cpu(dom, p, 5, 1, args.cpu_budget)
+        # the same step and warm-up counts as the reference arm
+        r = reference_cpu(dom, p, args.steps, args.warmup, args.cpu_budget)
         if "unavailable" not in r:
             out["cpu_baseline"] = {"value": r["value"], "unit": "Gcell/s", "cores": r["cores"],
                                    "kind": r["kind"], "sample": r["sample"]}

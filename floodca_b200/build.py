@@ -61,11 +61,18 @@ def _compile(src: Path, obj: Path, extra: list[str]) -> Path:
     return obj
 
 
+# The step kernels launch the full velocity pass from the device (a tail
+# launch, dynamic parallelism): their units are compiled as relocatable
+# device code and the core library links the device runtime.
+RDC_SRCS = {"wca_inst_f32.cu", "wca_inst_f32all.cu", "wca_inst_f64.cu"}
+
+
 def build(verbose: bool = True, jobs: int | None = None) -> dict[str, Path]:
     """Compiles every CUDA/C++ source and links the three libraries."""
     BUILD.mkdir(exist_ok=True)
     jobs = jobs or min(8, os.cpu_count() or 4)
-    tasks = [(CSRC / s, BUILD / (Path(s).stem + ".o"), []) for s in CORE_SRCS]
+    tasks = [(CSRC / s, BUILD / (Path(s).stem + ".o"), ["-rdc=true"] if s in RDC_SRCS else [])
+             for s in CORE_SRCS]
     tasks.append((CSRC / "abi_dropin.cpp", BUILD / "abi_dropin_f32.o", ["-x", "cu"]))
     tasks.append((CSRC / "abi_dropin.cpp", BUILD / "abi_dropin_f64.o", ["-x", "cu", "-DFCA_DOUBLE"]))
     with cf.ThreadPoolExecutor(jobs) as ex:
@@ -76,7 +83,7 @@ def build(verbose: bool = True, jobs: int | None = None) -> dict[str, Path]:
            "f64": PKG / "libfloodca_b200_f64.so"}
     link = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC"]
     if _deps_newer(out["core"], core_objs):
-        _run([*link, *map(str, core_objs), "-o", str(out["core"])])
+        _run([*link, *map(str, core_objs), "-lcudadevrt", "-o", str(out["core"])])
     for key, shim in (("f32", shim32), ("f64", shim64)):
         if _deps_newer(out[key], [shim, out["core"]]):
             _run([*link, str(shim), "-L", str(PKG), "-lfloodca_b200_core",

@@ -110,9 +110,11 @@ struct TimeCfg {
     double alpha_dx_d;
     int hyeto, max_steps, U, time_f32;
     int n_force_days, progress_every, inflow_ok, prec_f64;
-    int vseed_on;               // seed the dt pruning (the launcher adds the full pass)
+    int vseed_on;               // seed the dt pruning (a missed seed needs the full pass)
     int split;                  // slab of a row-split domain: the step control waits for
                                 // the velocity maximum reduced over all slabs
+    int tail_vpass;             // the step kernel itself tail-launches the full velocity
+                                // pass when its seed missed (else the launcher adds it)
 };
 
 // --------------------------------------------------------------------------
@@ -1188,6 +1190,12 @@ __host__ __device__ constexpr int step_blocks_per_sm()
                                               : step_min_blocks<K, CPL, MATH>();
 }
 
+template <typename T, int K, int MATH>
+__global__ void k_init_dt(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl, int only_if_needed);
+
+// CTAs of the full velocity pass (grid-stride over every cell; 256 threads)
+constexpr int VPASS_GRID = 148 * 8;
+
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
 __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
                                   step_blocks_per_sm<T, K, CPL, MATH, LANDONLY>()) k_step(GridD<T> g, RunK<T> rk, TimeCfg tc, Ctl *ctl,
@@ -1242,6 +1250,15 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
                 ctl->ctas_done = 0u;
             } else {
                 finalize<T>(ctl, tc, rk, true);
+                // a missed seed defers this step's dt to the full velocity
+                // pass: launched from here into the tail of the stream, so
+                // it runs before the next step and only when needed
+                if (tc.tail_vpass && ctl->need_v) {
+                    k_init_dt<T, K, MATH><<<VPASS_GRID, 256, 0, cudaStreamTailLaunch>>>(g, rk, tc,
+                                                                                      ctl, 1);
+                    if (cudaGetLastError() != cudaSuccess)
+                        ctl->err = 2;   // the host's poll runs the pass instead
+                }
             }
         }
     }

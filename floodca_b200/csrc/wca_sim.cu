@@ -298,7 +298,8 @@ extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *strea
     tc.U = cfg->U > 0 ? cfg->U : 1;
     tc.time_f32 = p == FCAB_PREC_F32_ALL;
     tc.prec_f64 = p == FCAB_PREC_F64;
-    tc.vseed_on = 1;        // sessions launch the full velocity pass after each step
+    tc.vseed_on = 1;        // seeded dt pruning; a missed seed is settled by the full
+    tc.tail_vpass = 1;      // velocity pass, which the step kernel launches itself
     *out = s;
     return 0;
 }
@@ -585,10 +586,14 @@ static void grid_view(FcabSim *s, GridD<T> &g)
     g.r_hi = s->cfg.nrows + s->hs;
 }
 
-// Kernel launches per step: the step, and with seeded dt pruning the
-// guarded full velocity pass (it returns at once unless the step deferred
-// its dt).
-static int launches_per_step(const FcabSim *s) { return s->tc.vseed_on ? 2 : 1; }
+// Host launches per step: the step; with seeded dt pruning and no tail
+// launch, also the guarded full velocity pass (it returns at once unless the
+// step deferred its dt). A tail-launched pass runs only when the seed missed
+// (FcabStats.dt_full_passes counts those).
+static int launches_per_step(const FcabSim *s)
+{
+    return s->tc.vseed_on && !s->tc.tail_vpass ? 2 : 1;
+}
 
 static cudaError_t launch_one(FcabSim *s)
 {
@@ -598,14 +603,14 @@ static cudaError_t launch_one(FcabSim *s)
         GridD<double> g;
         grid_view(s, g);
         e = s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
-        if (e == cudaSuccess && s->tc.vseed_on)
+        if (e == cudaSuccess && s->tc.vseed_on && !s->tc.tail_vpass)
             e = s->L.init(&g, &s->rkd, s->tc, s->ctl, full_grid, s->stream, 1);
         return e;
     }
     GridD<float> g;
     grid_view(s, g);
     e = s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
-    if (e == cudaSuccess && s->tc.vseed_on)
+    if (e == cudaSuccess && s->tc.vseed_on && !s->tc.tail_vpass)
         e = s->L.init(&g, &s->rkf, s->tc, s->ctl, full_grid, s->stream, 1);
     return e;
 }
@@ -695,10 +700,40 @@ extern "C" int fcab_sim_advance(FcabSim *s, int nsteps)
     return 0;
 }
 
+// Runs the guarded full velocity pass from the host (it does nothing unless
+// a step left its dt deferred).
+static int settle_deferred_dt(FcabSim *s)
+{
+    const int full_grid = 2 * 148 * 4;
+    cudaError_t e;
+    if (s->esize == 8) {
+        GridD<double> g;
+        grid_view(s, g);
+        e = s->L.init(&g, &s->rkd, s->tc, s->ctl, full_grid, s->stream, 1);
+    } else {
+        GridD<float> g;
+        grid_view(s, g);
+        e = s->L.init(&g, &s->rkf, s->tc, s->ctl, full_grid, s->stream, 1);
+    }
+    CUDA_TRY(e);
+    s->launches += 1;
+    return 0;
+}
+
 extern "C" int fcab_sim_poll(FcabSim *s, FcabPoll *p)
 {
     CUDA_TRY(cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (((const Ctl *)s->ctl_host)->need_v && !s->slab) {
+        // a deferred dt the step's tail launch did not settle (its launch
+        // failed): settle it here so the run goes on
+        int rc = settle_deferred_dt(s);
+        if (rc)
+            return rc;
+        CUDA_TRY(cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
     const Ctl *c = (const Ctl *)s->ctl_host;
     p->t = c->t;
     p->dt_base = c->dt_base;
@@ -889,6 +924,7 @@ extern "C" int fcab_sim_set_config(FcabSim *s, const FcabConfig *cfg)
     tc.U = cfg->U > 0 ? cfg->U : 1;
     tc.inflow_ok = inflow_ok;
     tc.vseed_on = 1;
+    tc.tail_vpass = 1;
     s->cpl = cfg->cols_per_lane ? pick_cpl(*cfg) : keep_cpl;
     s->variant_dirty = true;
     return 0;

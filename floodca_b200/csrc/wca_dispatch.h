@@ -21,7 +21,7 @@ struct VariantKey {
 // Type-erased launchers; `g`, `rk` point at GridD<T>/RunK<T> of the variant's T.
 struct Launchers {
     cudaError_t (*step)(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
-                        int warps_total, int grid, cudaStream_t s);
+                        int warps_total, int grid, cudaStream_t s, int smem);
     // full velocity pass + step control: the first step's dt, or
     // (only_if_needed) a dt deferred by a step whose pruned maximum fell
     // below its seed
@@ -29,6 +29,7 @@ struct Launchers {
                         cudaStream_t s, int only_if_needed);
     const void *step_fn;   // __global__ symbol, for occupancy queries
     int threads;           // threads per CTA of the step kernel
+    int tma_smem;          // dynamic shared memory of its TMA row source (0: none)
 };
 
 // Batched-ensemble launchers (FP32 state, FP64 accumulation).
@@ -76,9 +77,9 @@ bool lookup_f64(const VariantKey &k, Launchers *out);
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LAND>
 cudaError_t launch_step(const void *g, const void *rk, const TimeCfg &tc, Ctl *ctl,
-                        int warps_total, int grid, cudaStream_t s)
+                        int warps_total, int grid, cudaStream_t s, int smem)
 {
-    k_step<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, step_threads<CPL, MATH>(), 0, s>>>(
+    k_step<T, AccT, K, CPL, MATH, RAINF, LAND><<<grid, step_threads<CPL, MATH>(), smem, s>>>(
         *static_cast<const GridD<T> *>(g), *static_cast<const RunK<T> *>(rk), tc, ctl,
         warps_total);
     return cudaGetLastError();
@@ -102,6 +103,7 @@ Launchers make_launchers()
     L.init = &launch_init<T, K, MATH>;
     L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
     L.threads = step_threads<CPL, MATH>();
+    L.tma_smem = use_pair_sweep<T, CPL, LAND>() ? tma_smem_bytes(L.threads / 32) : 0;
     return L;
 }
 

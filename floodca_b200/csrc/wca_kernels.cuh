@@ -31,6 +31,8 @@
 // finish prepares the next step's control block.
 #pragma once
 
+#include <cuda.h>
+
 #include "wca_physics.cuh"
 
 namespace fcab {
@@ -59,6 +61,9 @@ struct GridD {
     long long pitch;
     int nr, nc;
     int r_lo, r_hi;             // rows of real cells: [0, nr), or with a slab's halo rows
+    // row-tile tensor maps of z, n, h0, h1 (device memory) for the TMA row
+    // source of the FP32 pair sweep, or nullptr (plain loads)
+    const CUtensorMap *tmap = nullptr;
 };
 
 // Uniform run constants.
@@ -1216,11 +1221,30 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
     if (wid >= warps_total)
         w0 = w1 = 0;
 
-    // step constants in shared memory for the pair sweep's exact re-evaluations
+    // step constants in shared memory for the pair sweep's exact
+    // re-evaluations; the warps' TMA rings and barriers (dynamic shared memory)
     __shared__ StepK<T> sk;
+    __shared__ uint32_t tphase[step_threads<CPL, MATH>() / 32];
+    __shared__ int tma_bad;
+    extern __shared__ __align__(1024) unsigned char fcab_dsm[];
+    uint32_t ring = 0u, bars = 0u;
+    const int wib = threadIdx.x >> 5;
     if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0) {
             sk = sv.k;
+            tma_bad = 0;
+        }
+        if (g.tmap) {
+            constexpr int W = step_threads<CPL, MATH>() / 32;
+            ring = smem_addr(fcab_dsm) + wib * TMA_WARP_B;
+            bars = smem_addr(fcab_dsm) + W * TMA_WARP_B + wib * TMA_NS * 8;
+            if (lane == 0) {
+                for (int q = 0; q < TMA_NS; q++)
+                    mbar_init1(bars + 8u * q);
+                tphase[wib] = 0u;
+                fence_proxy_async_smem();
+            }
+        }
         __syncthreads();
     }
     while (w0 < w1) {
@@ -1228,11 +1252,21 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
         const int r0 = (int)(w0 % nr);
         const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
         w0 += r1 - r0;
-        if constexpr (use_pair_sweep<T, CPL, LANDONLY>())
-            PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &sk, strip, r0, r1, lane, ss);
-        else
+        if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+            bool bad = false;
+            PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &sk, strip, r0, r1, lane, ss, ring,
+                                                 bars, &tphase[wib], &bad);
+            if (bad && lane == 0)
+                tma_bad = 1;
+        } else {
             sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane,
                                                                   ss);
+        }
+    }
+    if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+        __syncthreads();
+        if (threadIdx.x == 0 && tma_bad)
+            ctl->err = 3;           // a row tile never arrived; the host reports it
     }
 
     publish_sums<T, AccT, RAINF>(ss, sv, ctl, lane, wid & (NSLOT - 1));

@@ -257,7 +257,7 @@ extern "C" int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const flo
     }
     NA_TRY(L.init(&g, &rk, tc, ctl, nsm * 4, s, 0));
     for (int k = 0; k < cfg->max_steps; k++)
-        NA_TRY(L.step(&g, &rk, tc, ctl, grid * wpb, grid, s));
+        NA_TRY(L.step(&g, &rk, tc, ctl, grid * wpb, grid, s, 0));
     k_unpack<<<512, 256, 0, s>>>(g, ctl, h, hmax, tmax);
     NA_TRY(cudaGetLastError());
 

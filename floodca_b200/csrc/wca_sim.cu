@@ -5,7 +5,9 @@
 // own, and CUDA graphs of GRAPH_STEPS step launches that are replayed to
 // advance a run. The host only looks at the control block between chunks, to
 // end the run or to serve a pause (forcing-day reload, progress line).
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -108,6 +110,57 @@ __global__ void k_make_cr(const T *C, const T *R, const uint8_t *m, T *cr, long 
 }
 
 size_t esize_of(int prec) { return prec == FCAB_PREC_F64 ? 8 : 4; }
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// Row-tile maps of the padded FP32 fields z, n, h0, h1 for the pair sweep's
+// TMA row source: 2-D [rows][pitch] floats, boxes of 64 columns x TMA_RB
+// rows; rows past the array read as zeros (never used).
+bool make_row_maps(FcabSim *s)
+{
+    auto fn = tensor_map_encoder();
+    if (!fn || s->esize != 4)
+        return false;
+    CUtensorMap maps[4];
+    const void *fields[4] = {s->z, s->n, s->h0, s->h1};
+    cuuint64_t dims[2] = {(cuuint64_t)s->pitch, (cuuint64_t)s->rows_alloc};
+    cuuint64_t strides[1] = {(cuuint64_t)s->pitch * 4};
+    cuuint32_t box[2] = {64, (cuuint32_t)TMA_RB};
+    cuuint32_t es[2] = {1, 1};
+    for (int q = 0; q < 4; q++) {
+        if (((uintptr_t)fields[q] & 15) ||
+            fn(&maps[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)fields[q], dims, strides, box,
+               es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+                CUDA_SUCCESS)
+            return false;
+    }
+    if (fcab::cached_malloc(&s->tmaps, sizeof(maps)) != cudaSuccess)
+        return false;
+    return cudaMemcpyAsync(s->tmaps, maps, sizeof(maps), cudaMemcpyHostToDevice, s->stream) ==
+           cudaSuccess;
+}
+
+// Row source of the FP32 pair sweep: FCAB_ROW_SOURCE=tma streams rows by
+// TMA into shared memory, anything else (the default) by plain loads.
+bool want_tma_rows()
+{
+    const char *e = getenv("FCAB_ROW_SOURCE");
+    return e && strcmp(e, "tma") == 0;
+}
 
 }  // namespace
 
@@ -278,6 +331,8 @@ extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *strea
         fcab_sim_destroy(s);
         return fail(FCAB_ERR_CUDA, "allocation: %s", cudaGetErrorString(e));
     }
+    if (cfg->precision != FCAB_PREC_F64 && want_tma_rows())
+        s->use_tma = make_row_maps(s);
     if (cfg->precision == FCAB_PREC_F64)
         fill_runk<double>(s->rkd, *cfg);
     else
@@ -313,7 +368,7 @@ extern "C" void fcab_sim_destroy(FcabSim *s)
     if (s->stream)
         cudaStreamSynchronize(s->stream);
     void *ptrs[] = {s->z, s->n, s->cr, s->h0, s->h1, s->hmax, s->tmax, s->m, s->ctl,
-                    s->scratch, s->tmpC, s->tmpR};
+                    s->scratch, s->tmpC, s->tmpR, s->tmaps};
     for (void *q : ptrs)
         if (q)
             fcab::cached_free(q);
@@ -552,7 +607,12 @@ static int resolve_variant(FcabSim *s)
     // Grid: resident CTAs, or fewer so every warp streams >= seg_rows rows.
     int nsm = 0, per_sm = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->dev));
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->L.step_fn, s->L.threads, 0));
+    const int smem = s->use_tma ? s->L.tma_smem : 0;
+    if (smem > 0)
+        CUDA_TRY(cudaFuncSetAttribute(s->L.step_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, s->L.step_fn, s->L.threads,
+                                                           smem));
     if (per_sm < 1)
         per_sm = 1;
     const int wpb = s->L.threads / 32;     // warps per CTA
@@ -584,7 +644,11 @@ static void grid_view(FcabSim *s, GridD<T> &g)
     g.nc = s->cfg.ncols;
     g.r_lo = -s->hn;
     g.r_hi = s->cfg.nrows + s->hs;
+    g.tmap = s->use_tma && s->L.tma_smem > 0 ? static_cast<const CUtensorMap *>(s->tmaps)
+                                             : nullptr;
 }
+
+static int step_smem(const FcabSim *s) { return s->use_tma ? s->L.tma_smem : 0; }
 
 // Host launches per step: the step; with seeded dt pruning and no tail
 // launch, also the guarded full velocity pass (it returns at once unless the
@@ -602,14 +666,16 @@ static cudaError_t launch_one(FcabSim *s)
     if (s->esize == 8) {
         GridD<double> g;
         grid_view(s, g);
-        e = s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+        e = s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream,
+                      step_smem(s));
         if (e == cudaSuccess && s->tc.vseed_on && !s->tc.tail_vpass)
             e = s->L.init(&g, &s->rkd, s->tc, s->ctl, full_grid, s->stream, 1);
         return e;
     }
     GridD<float> g;
     grid_view(s, g);
-    e = s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream);
+    e = s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream,
+                  step_smem(s));
     if (e == cudaSuccess && s->tc.vseed_on && !s->tc.tail_vpass)
         e = s->L.init(&g, &s->rkf, s->tc, s->ctl, full_grid, s->stream, 1);
     return e;
@@ -1075,11 +1141,13 @@ extern "C" int fcab_sim_slab_step(FcabSim *s)
     if (s->esize == 8) {
         GridD<double> g;
         grid_view(s, g);
-        CUDA_TRY(s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream));
+        CUDA_TRY(s->L.step(&g, &s->rkd, s->tc, s->ctl, s->warps_total, s->grid, s->stream,
+                           step_smem(s)));
     } else {
         GridD<float> g;
         grid_view(s, g);
-        CUDA_TRY(s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream));
+        CUDA_TRY(s->L.step(&g, &s->rkf, s->tc, s->ctl, s->warps_total, s->grid, s->stream,
+                           step_smem(s)));
     }
     s->launches += 1;
     return 0;

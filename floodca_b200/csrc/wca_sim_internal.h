@@ -22,6 +22,8 @@ struct FcabSim {
     fcab::Ctl *ctl = nullptr;    // device control block
     void *ctl_host = nullptr;    // pinned mirror
     void *scratch = nullptr;     // 64 bytes of device scratch
+    void *tmaps = nullptr;       // row-tile tensor maps of z, n, h0, h1 (device memory)
+    bool use_tma = false;        // FP32 pair sweep rows by TMA
     fcab::RunK<float> rkf;
     fcab::RunK<double> rkd;
     fcab::TimeCfg tc;

@@ -29,8 +29,21 @@
 #pragma once
 
 #include "wca_f2.cuh"
+#include "wca_tma.cuh"
 
 namespace fcab {
+
+// TMA row source of the pair sweep: each warp streams its strip's z, h and
+// n rows through a ring of TMA_NS stages of TMA_RB rows (64 floats each),
+// filled by 2-D tensor loads and drained by shared-memory loads.
+constexpr int TMA_RB = 8, TMA_NS = 3;
+constexpr uint32_t TMA_FIELD_B = TMA_RB * 256, TMA_STAGE_B = 3 * TMA_FIELD_B;
+constexpr uint32_t TMA_WARP_B = TMA_NS * TMA_STAGE_B;
+// dynamic shared memory of a CTA of `warps` warps: rings, then barriers
+__host__ __device__ constexpr int tma_smem_bytes(int warps)
+{
+    return warps * (int)TMA_WARP_B + warps * TMA_NS * 8;
+}
 
 // Packed per-step constants of the pair sweep.
 struct PairK {
@@ -51,6 +64,12 @@ __device__ __forceinline__ f2 ld2_rw(const float *p)
 __device__ __forceinline__ void st2(float *p, f2 v)
 {
     *reinterpret_cast<float2 *>(p) = make_float2(lo2(v), hi2(v));
+}
+__device__ __forceinline__ f2 lds2(uint32_t a)
+{
+    float x, y;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(a));
+    return mk2(x, y);
 }
 
 // Discharge a -> b of two faces (one per half) between all-LAND cells with
@@ -235,11 +254,50 @@ struct PairSeg {
     int cbase, edges;                   // open edges: bit 0 N, 1 S, 2 W, 3 E (0: closed)
     bool out_lane, edge_strip, col0ok, col1ok;
     float thr, thr2c, T6;               // stage-E thresholds (warp-uniform)
+    // TMA row source
+    const CUtensorMap *tz, *th, *tn;    // tensor maps of z, the input depth, n
+    uint32_t ring, bars, srow;          // ring and barriers of the warp; next row's address
+    uint32_t *phase;                    // barrier phase bits of the warp (persist over segments)
+    int i0, blk, tx;                    // first row, current block, x of the strip
+    bool tma_err;
 };
 
 template <typename AccT, int K, int MATH, bool RAINF>
 struct PairSweep {
     using SS = StepSums<float, AccT>;
+
+    // ---- TMA row source
+    // lane 0: block b (rows i0 + 8b .. +7) of z, h, n into stage b % TMA_NS
+    static __device__ __forceinline__ void tma_issue(const PairSeg &G, int b)
+    {
+        const int st = b % TMA_NS;
+        const uint32_t bar = G.bars + 8u * st, dst = G.ring + st * TMA_STAGE_B;
+        const int y = G.i0 + b * TMA_RB + PADR;
+        mbar_arrive_tx(bar, TMA_STAGE_B);
+        tma_load_tile(dst, G.tz, bar, G.tx, y);
+        tma_load_tile(dst + TMA_FIELD_B, G.th, bar, G.tx, y);
+        tma_load_tile(dst + 2 * TMA_FIELD_B, G.tn, bar, G.tx, y);
+    }
+    static __device__ __forceinline__ void tma_wait(PairSeg &G, int b)
+    {
+        const int st = b % TMA_NS;
+        if (!mbar_wait_bounded(G.bars + 8u * st, (*G.phase >> st) & 1u))
+            G.tma_err = true;
+        *G.phase ^= 1u << st;
+    }
+    // moves to block b: refills the stage of block b-1 (all lanes are past
+    // it) with block b + TMA_NS - 1, then waits for block b
+    static __device__ __forceinline__ void tma_turn(PairSeg &G, int lane)
+    {
+        const int b = ++G.blk;
+        __syncwarp();
+        if (lane == 0) {
+            fence_proxy_async_smem();
+            tma_issue(G, b + TMA_NS - 1);
+        }
+        tma_wait(G, b);
+        G.srow = G.ring + (b % TMA_NS) * TMA_STAGE_B + lane * 8;
+    }
 
     // thr = max(warp maximum so far, seed); thr2c = thr^2 (1 - 1e-6) for the
     // critical-velocity prefilter; T6 = thr^6 (1 - 2e-4) for the bound (0 when
@@ -254,10 +312,10 @@ struct PairSweep {
     }
 
     // one iteration of the pipeline; J = (i - i0) & 3
-    template <int J>
+    template <int J, bool TMA>
     static __device__ __forceinline__ void iter(PairRing<K> &R, PairSeg &G, const PairK &c,
                                                 const StepVals<float> &sv, const RunK<float> &rk,
-                                                const StepK<float> *kp, SS &ss, int i)
+                                                const StepK<float> *kp, SS &ss, int i, int lane)
     {
         constexpr int S1 = (J + 1) & 3;   // row i+1
         constexpr int S0 = J & 3;         // row i
@@ -271,14 +329,25 @@ struct PairSweep {
         // ---- loads: row i+1, and hmax / rain field of row i-1
         {
             const long long off = (long long)(i + 1 + PADR) * pitch + G.colo;
-            R.z[S1] = ld2(G.gz + off);
-            R.h[S1] = ld2(G.hin + off);
-            R.n[S1] = ld2(G.gn + off);
-            const int ra = min(i + 1 + PF_ROWS, G.nr + PADR - 1);
-            const long long offa = (long long)(ra + PADR) * pitch + G.colo;
-            prefetch_l2(G.gz + offa);
-            prefetch_l2(G.hin + offa);
-            prefetch_l2(G.gn + offa);
+            if constexpr (TMA) {
+                // row i+1 is row i+1-i0 of the stream: a new block every 8
+                // rows, which (8 being a multiple of 4) only J = 3 can meet
+                if (J == 3 && ((i + 1 - G.i0) & (TMA_RB - 1)) == 0)
+                    tma_turn(G, lane);
+                R.z[S1] = lds2(G.srow);
+                R.h[S1] = lds2(G.srow + TMA_FIELD_B);
+                R.n[S1] = lds2(G.srow + 2 * TMA_FIELD_B);
+                G.srow += 256;
+            } else {
+                R.z[S1] = ld2(G.gz + off);
+                R.h[S1] = ld2(G.hin + off);
+                R.n[S1] = ld2(G.gn + off);
+                const int ra = min(i + 1 + PF_ROWS, G.nr + PADR - 1);
+                const long long offa = (long long)(ra + PADR) * pitch + G.colo;
+                prefetch_l2(G.gz + offa);
+                prefetch_l2(G.hin + offa);
+                prefetch_l2(G.gn + offa);
+            }
             const long long off1 = off - 2 * pitch;
             if (G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1)
                 R.hm[Sm1] = ld2_rw(G.ghmax + off1);
@@ -598,10 +667,25 @@ struct PairSweep {
     }
 
     // One warp streams output rows [r0, r1) of one strip (as sweep_segment).
-    // kp: the step constants in shared memory, for the exact re-evaluations.
-    static __device__ void run(const GridD<float> &g, const RunK<float> &rk,
+    // kp: the step constants in shared memory, for the exact re-evaluations;
+    // ring, bars, phase: the warp's TMA ring, barriers and phase bits (the
+    // rows come by TMA when the grid has tensor maps, else by plain loads).
+    static __device__ __forceinline__ void run(const GridD<float> &g, const RunK<float> &rk,
                                const StepVals<float> &sv, const StepK<float> *kp, int strip, int r0,
-                               int r1, int lane, SS &ss)
+                               int r1, int lane, SS &ss, uint32_t ring = 0u, uint32_t bars = 0u,
+                               uint32_t *phase = nullptr, bool *tma_err = nullptr)
+    {
+        if (g.tmap && ring)
+            run_impl<true>(g, rk, sv, kp, strip, r0, r1, lane, ss, ring, bars, phase, tma_err);
+        else
+            run_impl<false>(g, rk, sv, kp, strip, r0, r1, lane, ss, 0u, 0u, nullptr, nullptr);
+    }
+
+    template <bool TMA>
+    static __device__ __forceinline__ void run_impl(const GridD<float> &g, const RunK<float> &rk,
+                                    const StepVals<float> &sv, const StepK<float> *kp, int strip,
+                                    int r0, int r1, int lane, SS &ss, uint32_t ring, uint32_t bars,
+                                    uint32_t *phase, bool *tma_err)
     {
         using Gm = Geom<2>;
         PairSeg G;
@@ -658,6 +742,8 @@ struct PairSweep {
         // iterations compute rows above the segment's halo only
         const int n_it = ((r1 - r0 + 6) + 3) & ~3;
         const int i0 = r1 + 3 - n_it;
+        G.i0 = i0;
+        G.tma_err = false;
 
         PairRing<K> R;
         const f2 z0 = bc2(0.0f);
@@ -673,17 +759,47 @@ struct PairSweep {
             R.Ln[q] = bc2(__int_as_float(0x7fc00000));
             R.ko[q] = R.ef[q] = 0u;
         }
-        {
+        if constexpr (TMA) {
+            G.tz = g.tmap;
+            G.tn = g.tmap + 1;
+            G.th = g.tmap + (sv.hin == g.h1 ? 3 : 2);
+            G.ring = ring;
+            G.bars = bars;
+            G.phase = phase;
+            G.tx = strip * Gm::OW - Gm::HL + PADC;      // a multiple of 4 floats
+            G.blk = 0;
+            __syncwarp();
+            if (lane == 0) {
+                fence_proxy_async_smem();
+                for (int b = 0; b < TMA_NS; b++)
+                    tma_issue(G, b);
+            }
+            tma_wait(G, 0);
+            G.srow = G.ring + lane * 8;
+            R.z[0] = lds2(G.srow);
+            R.h[0] = lds2(G.srow + TMA_FIELD_B);
+            R.n[0] = lds2(G.srow + 2 * TMA_FIELD_B);
+            G.srow += 256;
+        } else {
             const long long off = (long long)(i0 + PADR) * G.pitch + G.colo;
             R.z[0] = ld2(G.gz + off);
             R.h[0] = ld2(G.hin + off);
             R.n[0] = ld2(G.gn + off);
         }
         for (int i = i0; i < i0 + n_it; i += 4) {
-            iter<0>(R, G, c, sv, rk, kp, ss, i);
-            iter<1>(R, G, c, sv, rk, kp, ss, i + 1);
-            iter<2>(R, G, c, sv, rk, kp, ss, i + 2);
-            iter<3>(R, G, c, sv, rk, kp, ss, i + 3);
+            iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
+            iter<1, TMA>(R, G, c, sv, rk, kp, ss, i + 1, lane);
+            iter<2, TMA>(R, G, c, sv, rk, kp, ss, i + 2, lane);
+            iter<3, TMA>(R, G, c, sv, rk, kp, ss, i + 3, lane);
+        }
+        if constexpr (TMA) {
+            // no load may still be writing the ring when the next segment
+            // starts: wait for the blocks issued ahead
+            for (int b = G.blk + 1; b < G.blk + TMA_NS; b++)
+                tma_wait(G, b);
+            __syncwarp();
+            if (G.tma_err && tma_err)
+                *tma_err = true;
         }
         // uniform rain on LAND output cells, counted per lane
         if constexpr (sizeof(AccT) == 8 && !RAINF) {

@@ -1261,7 +1261,13 @@ __global__ void k_math_probe(int which, const float *x, const float *y, float *o
             r = __frcp_rn(x[i]);
         else if (which == 8)
             r = __fsqrt_rn(x[i]);
-        else
+        else if (which == 10) {
+            // the pair sweep's cube root: its value where it decides the
+            // rounding itself, NaN where it defers to the exact evaluation
+            bool u0, u1;
+            const f2 c = cbrt_sq2(mk2(x[i], x[i]), u0, u1);
+            r = u0 ? __int_as_float(0x7fc00000) : lo2(c);
+        } else
             r = __fdiv_rn(x[i], y[i]);
         out[i] = r;
     }

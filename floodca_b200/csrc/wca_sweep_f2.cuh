@@ -37,6 +37,13 @@ namespace fcab {
 // n rows through a ring of TMA_NS stages of TMA_RB rows (64 floats each),
 // filled by 2-D tensor loads and drained by shared-memory loads.
 constexpr int TMA_RB = 8, TMA_NS = 3;
+
+// Iterations per pass of the pair sweep's loop: 4 unrolls the body over the
+// four ring slots (no register copies, four copies of the code); 1 runs one
+// body and rotates the ring's registers after each row (a smaller loop).
+#ifndef FCAB_PAIR_UNROLL
+#define FCAB_PAIR_UNROLL 4
+#endif
 constexpr uint32_t TMA_FIELD_B = TMA_RB * 256, TMA_STAGE_B = 3 * TMA_FIELD_B;
 constexpr uint32_t TMA_WARP_B = TMA_NS * TMA_STAGE_B;
 // dynamic shared memory of a CTA of `warps` warps: rings, then barriers
@@ -260,7 +267,32 @@ struct PairSeg {
     uint32_t *phase;                    // barrier phase bits of the warp (persist over segments)
     int i0, blk, tx;                    // first row, current block, x of the strip
     bool tma_err;
+    long long o1;                       // element offset of row i+1 in the current iteration
 };
+
+// The ring viewed one row further: slot q takes slot q+1's registers.
+template <typename V>
+__device__ __forceinline__ void rot4(V (&a)[4])
+{
+    const V t = a[0];
+    a[0] = a[1];
+    a[1] = a[2];
+    a[2] = a[3];
+    a[3] = t;
+}
+template <int K>
+__device__ __forceinline__ void rotate_ring(PairRing<K> &R)
+{
+    rot4(R.z); rot4(R.h); rot4(R.n); rot4(R.L);
+    rot4(R.Xp); rot4(R.Xn); rot4(R.Yp); rot4(R.Yn);
+    rot4(R.s); rot4(R.Qy); rot4(R.hn); rot4(R.Ln); rot4(R.n6);
+    rot4(R.hm); rot4(R.cr); rot4(R.qo); rot4(R.ko); rot4(R.ef);
+    if constexpr (K == 8) {
+        rot4(R.zr); rot4(R.hr); rot4(R.nr); rot4(R.Lr);
+        rot4(R.Ep); rot4(R.En); rot4(R.Wp); rot4(R.Wn);
+        rot4(R.Qe); rot4(R.Qw);
+    }
+}
 
 template <typename AccT, int K, int MATH, bool RAINF>
 struct PairSweep {
@@ -328,11 +360,13 @@ struct PairSweep {
 
         // ---- loads: row i+1, and hmax / rain field of row i-1
         {
-            const long long off = (long long)(i + 1 + PADR) * pitch + G.colo;
+            const long long off = G.o1;
+            G.o1 += pitch;
             if constexpr (TMA) {
                 // row i+1 is row i+1-i0 of the stream: a new block every 8
-                // rows, which (8 being a multiple of 4) only J = 3 can meet
-                if (J == 3 && ((i + 1 - G.i0) & (TMA_RB - 1)) == 0)
+                // rows, which (8 being a multiple of 4) an unrolled pass
+                // only meets at J = 3
+                if ((FCAB_PAIR_UNROLL == 1 || J == 3) && ((i + 1 - G.i0) & (TMA_RB - 1)) == 0)
                     tma_turn(G, lane);
                 R.z[S1] = lds2(G.srow);
                 R.h[S1] = lds2(G.srow + TMA_FIELD_B);
@@ -342,8 +376,10 @@ struct PairSweep {
                 R.z[S1] = ld2(G.gz + off);
                 R.h[S1] = ld2(G.hin + off);
                 R.n[S1] = ld2(G.gn + off);
-                const int ra = min(i + 1 + PF_ROWS, G.nr + PADR - 1);
-                const long long offa = (long long)(ra + PADR) * pitch + G.colo;
+                const long long offa =
+                    i + 1 + PF_ROWS <= G.nr + PADR - 1
+                        ? off + PF_ROWS * pitch
+                        : (long long)(G.nr + 2 * PADR - 1) * pitch + G.colo;
                 prefetch_l2(G.gz + offa);
                 prefetch_l2(G.hin + offa);
                 prefetch_l2(G.gn + offa);
@@ -601,7 +637,7 @@ struct PairSweep {
             const bool rise0 = cell0 && lo2(hu) > lo2(hmo);
             const bool rise1 = cell1 && hi2(hu) > hi2(hmo);
             if (row_out && G.out_lane) {
-                const long long off2 = (long long)(r + PADR) * pitch + G.colo;
+                const long long off2 = G.o1 - 4 * pitch;        // row i-2
                 st2(G.hout + off2, hkeep);
                 if (rise0 || rise1) {
                     st2(G.ghmax + off2, sel2(rise0, rise1, hu, hmo));
@@ -632,7 +668,7 @@ struct PairSweep {
                 const bool erow = (r == 0 && (G.edges & 1)) || (r == G.nr - 1 && (G.edges & 2));
                 if (erow || G.edge_strip) {
                     // the open virtual neighbour z - S_bnd*dx, h = 0 (physics.h:183-189)
-                    const long long off3 = (long long)(r + PADR) * pitch + G.colo;
+                    const long long off3 = G.o1 - 5 * pitch;    // row i-3
                     const f2 z3 = ld2(G.gz + off3);
                     const f2 dv = abs2(sub2(la, sub2(z3, bc2(sv.k.S_bnd * sv.k.dx))));
 #pragma unroll
@@ -655,7 +691,7 @@ struct PairSweep {
             const bool x0 = (ef & 1u) && (lo2(lhs) >= lo2(rhs) || lo2(lhs) < 1e-30f);
             const bool x1 = (ef & 2u) && (hi2(lhs) >= hi2(rhs) || hi2(lhs) < 1e-30f);
             if (__any_sync(0xffffffffu, x0 || x1)) {
-                const long long off3 = (long long)(r + PADR) * pitch + G.colo;
+                const long long off3 = G.o1 - 5 * pitch;        // row i-3
                 const f2 n3 = ld2(G.gn + off3);
                 float vm = ss.vmax;
                 if (x0 || x1)
@@ -786,11 +822,19 @@ struct PairSweep {
             R.h[0] = ld2(G.hin + off);
             R.n[0] = ld2(G.gn + off);
         }
-        for (int i = i0; i < i0 + n_it; i += 4) {
-            iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
-            iter<1, TMA>(R, G, c, sv, rk, kp, ss, i + 1, lane);
-            iter<2, TMA>(R, G, c, sv, rk, kp, ss, i + 2, lane);
-            iter<3, TMA>(R, G, c, sv, rk, kp, ss, i + 3, lane);
+        G.o1 = (long long)(i0 + 1 + PADR) * G.pitch + G.colo;
+        if constexpr (FCAB_PAIR_UNROLL == 1) {
+            for (int i = i0; i < i0 + n_it; i++) {
+                iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
+                rotate_ring<K>(R);
+            }
+        } else {
+            for (int i = i0; i < i0 + n_it; i += 4) {
+                iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
+                iter<1, TMA>(R, G, c, sv, rk, kp, ss, i + 1, lane);
+                iter<2, TMA>(R, G, c, sv, rk, kp, ss, i + 2, lane);
+                iter<3, TMA>(R, G, c, sv, rk, kp, ss, i + 3, lane);
+            }
         }
         if constexpr (TMA) {
             // no load may still be writing the ring when the next segment

@@ -109,6 +109,27 @@ def test_device_cube_root_is_correctly_rounded():
     assert bad.size <= 2, (bad.size, x[bad[:5]], out[bad[:5]], want[bad[:5]])
 
 
+def test_packed_cube_root_decides_only_correct_roundings():
+    """The pair sweep's hf^(2/3) (probe 10): wherever it decides the rounding
+    itself it equals the exact evaluation (probe 0), and it defers only a
+    small share of inputs."""
+    from floodca_b200.lib import core
+    rng = np.random.default_rng(9)
+    x = np.concatenate([
+        np.float32(2.0) ** rng.uniform(-20, 20, 4_000_000).astype(np.float32),
+        np.linspace(1e-3, 10.0, 1_000_000, dtype=np.float32),
+        np.float32(2.0) ** np.arange(-20, 21).astype(np.float32),
+    ]).astype(np.float32)
+    fast, exact = np.empty_like(x), np.empty_like(x)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert core().fcab_math_probe(10, vp(x), None, vp(fast), x.size, 9.81) == 0
+    assert core().fcab_math_probe(0, vp(x), None, vp(exact), x.size, 9.81) == 0
+    decided = ~np.isnan(fast)
+    bad = np.flatnonzero(decided & (fast != exact))
+    assert bad.size == 0, (bad.size, x[bad[:5]], fast[bad[:5]], exact[bad[:5]])
+    assert decided.mean() > 0.995
+
+
 def test_device_critical_velocity_min_is_exact():
     from floodca_b200.lib import core
     rng = np.random.default_rng(8)

@@ -1234,10 +1234,14 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
             sk = sv.k;
             tma_bad = 0;
         }
+        // TMA destinations must start on 128-byte boundaries: the rings
+        // start at the dynamic area rounded up to 1024 bytes (the area has
+        // 1 KB of slack for it)
+        const uint32_t dbase = (smem_addr(fcab_dsm) + 1023u) & ~1023u;
         if (g.tmap) {
             constexpr int W = step_threads<CPL, MATH>() / 32;
-            ring = smem_addr(fcab_dsm) + wib * TMA_WARP_B;
-            bars = smem_addr(fcab_dsm) + W * TMA_WARP_B + wib * TMA_NS * 8;
+            ring = dbase + wib * TMA_WARP_B;
+            bars = dbase + W * TMA_WARP_B + wib * TMA_NS * 8;
             if (lane == 0) {
                 for (int q = 0; q < TMA_NS; q++)
                     mbar_init1(bars + 8u * q);

@@ -46,10 +46,13 @@ constexpr int TMA_RB = 8, TMA_NS = 3;
 #endif
 constexpr uint32_t TMA_FIELD_B = TMA_RB * 256, TMA_STAGE_B = 3 * TMA_FIELD_B;
 constexpr uint32_t TMA_WARP_B = TMA_NS * TMA_STAGE_B;
-// dynamic shared memory of a CTA of `warps` warps: rings, then barriers
+// dynamic shared memory of a CTA of `warps` warps: 1 KB of slack to round
+// the start up to a 1024-byte boundary (the dynamic area follows the static
+// shared variables, so its own start is only 16-byte aligned), the rings,
+// then the barriers
 __host__ __device__ constexpr int tma_smem_bytes(int warps)
 {
-    return warps * (int)TMA_WARP_B + warps * TMA_NS * 8;
+    return 1024 + warps * (int)TMA_WARP_B + warps * TMA_NS * 8;
 }
 
 // Packed per-step constants of the pair sweep.

@@ -29,8 +29,10 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false keeps a*b+c as two rounded operations, as the reference's
 # parity build does on the host (-ffp-contract=off); explicit fmaf() calls
-# in the kernels are unaffected.
-NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
+# in the kernels are unaffected. ptxas takes its own --fmad=false: without it
+# a packed mul.rn.f32x2 feeding a packed add.rn.f32x2 was fused on sm_100a.
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xptxas", "--fmad=false",
+           "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC),
            *os.environ.get("FCAB_NVCC_FLAGS", "").split()]
 

@@ -1183,15 +1183,25 @@ __host__ __device__ constexpr int step_min_blocks()
                             : CPL == 2 ? (MATH == MATH_EXACT && K == 4 ? 16 : 12) : 8)) /
            (step_threads<CPL, MATH>() / 32);
 }
-// Resident warps per SM the pair sweep's register allocation aims for: at 8
-// (up to 255 registers) its four-row ring of packed pairs needs no spills.
+// Resident warps per SM the pair sweep's register allocation aims for (168
+// registers at 12). Measured at 4096^2 on a B200 (one-row loop): 12 warps
+// 33.9 Gcell/s against 26.0 at 8 (255 registers, no spills).
 #ifndef FCAB_PAIR_WARPS
-#define FCAB_PAIR_WARPS 8
+#define FCAB_PAIR_WARPS 12
 #endif
+// K = 8 holds twice the face state: 8 warps (up to 255 registers, no spills)
+#ifndef FCAB_PAIR_WARPS_K8
+#define FCAB_PAIR_WARPS_K8 8
+#endif
+template <int K>
+__host__ __device__ constexpr int pair_warps()
+{
+    return K == 8 ? FCAB_PAIR_WARPS_K8 : FCAB_PAIR_WARPS;
+}
 template <typename T, int K, int CPL, int MATH, bool LANDONLY>
 __host__ __device__ constexpr int step_blocks_per_sm()
 {
-    return use_pair_sweep<T, CPL, LANDONLY>() ? FCAB_PAIR_WARPS / (step_threads<CPL, MATH>() / 32)
+    return use_pair_sweep<T, CPL, LANDONLY>() ? pair_warps<K>() / (step_threads<CPL, MATH>() / 32)
                                               : step_min_blocks<K, CPL, MATH>();
 }
 
@@ -1328,7 +1338,7 @@ struct BatchQ {
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128, use_pair_sweep<T, CPL, LANDONLY>() ? FCAB_PAIR_WARPS / 4
+__global__ void __launch_bounds__(128, use_pair_sweep<T, CPL, LANDONLY>() ? pair_warps<K>() / 4
                                                                       : (CPL == 2 ? 4 : 1))
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,

@@ -1267,6 +1267,9 @@ __global__ void k_math_probe(int which, const float *x, const float *y, float *o
             bool u0, u1;
             const f2 c = cbrt_sq2(mk2(x[i], x[i]), u0, u1);
             r = u0 ? __int_as_float(0x7fc00000) : lo2(c);
+        } else if (which == 11) {
+            // a packed product then a packed sum: two roundings, RN(RN(x*y) + g)
+            r = lo2(add2(mul2(mk2(x[i], x[i]), mk2(y[i], y[i])), bc2(g)));
         } else
             r = __fdiv_rn(x[i], y[i]);
         out[i] = r;

@@ -396,7 +396,8 @@ FCAB_API int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const float
  * hf^(2/3); 1: min(x, RN(sqrt(g*y))); 2: the fast-mode hf^(2/3); 4/5/6: the
  * branch-free reciprocal, square root and Markstein quotient x/y; 7/8/9: the
  * IEEE reciprocal, square root and quotient they must equal; 10: the packed
- * pair sweep's hf^(2/3), NaN where it defers to the exact evaluation. */
+ * pair sweep's hf^(2/3), NaN where it defers to the exact evaluation; 11: a
+ * packed product then a packed sum, RN(RN(x*y) + g), rounded twice. */
 FCAB_API int fcab_math_probe(int which, const float *x, const float *y, float *out, long long n,
                              float g);
 

@@ -130,6 +130,23 @@ def test_packed_cube_root_decides_only_correct_roundings():
     assert decided.mean() > 0.995
 
 
+def test_packed_product_then_sum_rounds_twice():
+    """A packed multiply feeding a packed add must not be contracted into a
+    fused multiply-add (the reference rounds the product, then the sum)."""
+    from floodca_b200.lib import core
+    rng = np.random.default_rng(10)
+    x = rng.uniform(0.5, 2.0, 1_000_000).astype(np.float32)
+    y = rng.uniform(1e-7, 1e-5, x.size).astype(np.float32)
+    g = np.float32(8.333334e-4)
+    out = np.empty_like(x)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert core().fcab_math_probe(11, vp(x), vp(y), vp(out), x.size, g) == 0
+    want = (x * y).astype(np.float32) + g
+    fused = (x.astype(np.float64) * y.astype(np.float64) + np.float64(g)).astype(np.float32)
+    assert np.count_nonzero(want != fused) > 1000      # the two differ often here
+    assert np.array_equal(out, want)
+
+
 def test_device_critical_velocity_min_is_exact():
     from floodca_b200.lib import core
     rng = np.random.default_rng(8)

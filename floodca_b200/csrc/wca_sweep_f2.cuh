@@ -244,9 +244,9 @@ template <int K>
 struct PairRing {
     f2 z[4], h[4], n[4], L[4];          // row data, old level z + h
     f2 zr[4], hr[4], nr[4], Lr[4];      // right-shifted copies (K = 8 SW faces)
-    f2 Xp[4], Xn[4];                    // x faces (c -> c+1) of a row, positive / negative part
-    f2 Yp[4], Yn[4];                    // y faces (r -> r+1), by the upper row
-    f2 Ep[4], En[4], Wp[4], Wn[4];      // K = 8: SE (r,c)->(r+1,c+1), SW (r,c+1)->(r+1,c)
+    f2 X[4];                            // x faces (c -> c+1) of a row
+    f2 Y[4];                            // y faces (r -> r+1), by the upper row
+    f2 E[4], W[4];                      // K = 8: SE (r,c)->(r+1,c+1), SW (r,c+1)->(r+1,c)
     f2 s[4];                            // limiter
     f2 Qy[4], Qe[4], Qw[4];             // scaled y / SE / SW discharges, by the upper row
     f2 hn[4], Ln[4], n6[4];             // new depth, new level (NaN outside the grid), n^6
@@ -288,12 +288,12 @@ template <int K>
 __device__ __forceinline__ void rotate_ring(PairRing<K> &R)
 {
     rot4(R.z); rot4(R.h); rot4(R.n); rot4(R.L);
-    rot4(R.Xp); rot4(R.Xn); rot4(R.Yp); rot4(R.Yn);
+    rot4(R.X); rot4(R.Y);
     rot4(R.s); rot4(R.Qy); rot4(R.hn); rot4(R.Ln); rot4(R.n6);
     rot4(R.hm); rot4(R.cr); rot4(R.qo); rot4(R.ko); rot4(R.ef);
     if constexpr (K == 8) {
         rot4(R.zr); rot4(R.hr); rot4(R.nr); rot4(R.Lr);
-        rot4(R.Ep); rot4(R.En); rot4(R.Wp); rot4(R.Wn);
+        rot4(R.E); rot4(R.W);
         rot4(R.Qe); rot4(R.Qw);
     }
 }
@@ -471,15 +471,11 @@ struct PairSweep {
                         ss.capn += (unsigned)ue0 + (unsigned)ue1 + (unsigned)uw0 + (unsigned)uw1;
                 }
             }
-            R.Xp[S0] = max2(X, z0);
-            R.Xn[S0] = min2(X, z0);
-            R.Yp[Sm1] = max2(Y, z0);
-            R.Yn[Sm1] = min2(Y, z0);
+            R.X[S0] = X;
+            R.Y[Sm1] = Y;
             if constexpr (K == 8) {
-                R.Ep[Sm1] = max2(E, z0);
-                R.En[Sm1] = min2(E, z0);
-                R.Wp[Sm1] = max2(W, z0);
-                R.Wn[Sm1] = min2(W, z0);
+                R.E[Sm1] = E;
+                R.W[Sm1] = W;
             }
         }
 
@@ -488,14 +484,15 @@ struct PairSweep {
         //      d2+, d2-, open slots
         {
             const int r = i - 1;
-            f2 out = sub2(R.Xp[Sm1], left2(R.Xn[Sm1]));
-            out = add2(out, R.Yp[Sm1]);
-            out = sub2(out, R.Yn[Sm2]);
+            // max(Q, 0) of the faces leaving, -min(Q, 0) of the faces entering
+            f2 out = sub2(max2(R.X[Sm1], z0), min2(left2(R.X[Sm1]), z0));
+            out = add2(out, max2(R.Y[Sm1], z0));
+            out = sub2(out, min2(R.Y[Sm2], z0));
             if constexpr (K == 8) {
-                out = add2(out, R.Ep[Sm1]);
-                out = sub2(out, left2(R.En[Sm2]));
-                out = add2(out, left2(R.Wp[Sm1]));
-                out = sub2(out, R.Wn[Sm2]);
+                out = add2(out, max2(R.E[Sm1], z0));
+                out = sub2(out, min2(left2(R.E[Sm2]), z0));
+                out = add2(out, max2(left2(R.W[Sm1]), z0));
+                out = sub2(out, min2(R.W[Sm2], z0));
             }
             R.ko[Sm1] = 0u;
             if (G.edges) {
@@ -535,16 +532,17 @@ struct PairSweep {
             const bool row_out = r >= G.r0 && r < G.r1;
             const f2 s0 = R.s[Sm2];
             const f2 sr = right2(s0);
-            const f2 Qsx = fma2(R.Xn[Sm2], sr, mul2(R.Xp[Sm2], s0));
-            const f2 Qsy = fma2(R.Yn[Sm2], R.s[Sm1], mul2(R.Yp[Sm2], s0));
+            const f2 Qsx = fma2(min2(R.X[Sm2], z0), sr, mul2(max2(R.X[Sm2], z0), s0));
+            const f2 Qsy = fma2(min2(R.Y[Sm2], z0), R.s[Sm1], mul2(max2(R.Y[Sm2], z0), s0));
             R.Qy[Sm2] = Qsy;
             f2 net = sub2(z0, Qsx);
             net = add2(net, left2(Qsx));
             net = sub2(net, Qsy);
             net = add2(net, R.Qy[Sm3]);
             if constexpr (K == 8) {
-                const f2 Qse = fma2(R.En[Sm2], right2(R.s[Sm1]), mul2(R.Ep[Sm2], s0));
-                const f2 Qsw = fma2(R.Wn[Sm2], R.s[Sm1], mul2(R.Wp[Sm2], sr));
+                const f2 Qse = fma2(min2(R.E[Sm2], z0), right2(R.s[Sm1]),
+                                    mul2(max2(R.E[Sm2], z0), s0));
+                const f2 Qsw = fma2(min2(R.W[Sm2], z0), R.s[Sm1], mul2(max2(R.W[Sm2], z0), sr));
                 R.Qe[Sm2] = Qse;
                 R.Qw[Sm2] = Qsw;
                 net = sub2(net, Qse);
@@ -791,8 +789,7 @@ struct PairSweep {
         for (int q = 0; q < 4; q++) {
             R.z[q] = R.h[q] = R.n[q] = R.L[q] = z0;
             R.zr[q] = R.hr[q] = R.nr[q] = R.Lr[q] = z0;
-            R.Xp[q] = R.Xn[q] = R.Yp[q] = R.Yn[q] = z0;
-            R.Ep[q] = R.En[q] = R.Wp[q] = R.Wn[q] = z0;
+            R.X[q] = R.Y[q] = R.E[q] = R.W[q] = z0;
             R.s[q] = bc2(1.0f);
             R.Qy[q] = R.Qe[q] = R.Qw[q] = z0;
             R.hn[q] = R.n6[q] = R.hm[q] = R.cr[q] = R.qo[q] = z0;

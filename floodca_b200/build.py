@@ -29,9 +29,10 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false keeps a*b+c as two rounded operations, as the reference's
 # parity build does on the host (-ffp-contract=off); explicit fmaf() calls
-# in the kernels are unaffected. ptxas takes its own --fmad=false: without it
-# a packed mul.rn.f32x2 feeding a packed add.rn.f32x2 was fused on sm_100a.
-NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xptxas", "--fmad=false",
+# in the kernels are unaffected. It does not stop ptxas from fusing a packed
+# mul.rn.f32x2 into a following add.rn.f32x2 (nor does ptxas's own
+# --fmad=false); the pair sweep forms such products with scalar mul.rn.
+NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false",
            "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(INCLUDE), "-I", str(CSRC),
            *os.environ.get("FCAB_NVCC_FLAGS", "").split()]

@@ -251,6 +251,8 @@ extern "C" int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *
         fcab_sim_destroy(s);
         return -2;
     }
+    if (rc == 1)
+        acc->t = (double)cfg->T_sim;   // a forcing day failed to load: the run ends there
     acc->force_day = p.force_day;
     ti = now_s();
     if (fcab_sim_download(s, g->h, g->hmax, g->tmax) != 0) {
@@ -323,7 +325,8 @@ extern "C" int fca_cuda_ens_run(FcaCudaEns *e, FcaGrid *g, const FcaRunCfg *cfg,
     tm->t_dt = tm->t_flux = tm->t_limiter = tm->t_update = -1;
     const int step0 = acc->step;
     const double t_wall0 = now_s();
-    if (drive(e->s, g, cfg, acc, tm, poll, pctx, poll_every, t_wall0) < 0) {
+    const int rc = drive(e->s, g, cfg, acc, tm, poll, pctx, poll_every, t_wall0);
+    if (rc < 0) {
         report("ens_run");
         return -2;
     }
@@ -333,6 +336,8 @@ extern "C" int fca_cuda_ens_run(FcaCudaEns *e, FcaGrid *g, const FcaRunCfg *cfg,
     tm->wall_total += now_s() - t_wall0;
     if (collect(e->s, acc, step0) != 0)
         return -2;
+    if (rc == 1)
+        acc->t = (double)cfg->T_sim;
     acc->force_day = p.force_day;
     ti = now_s();
     long long fl[4] = {0, 0, 0, 0};

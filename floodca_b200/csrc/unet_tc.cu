@@ -62,12 +62,13 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
     return ok != 0;
 }
 
-// Waits for the phase with the given parity; gives up after about 2 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+// Waits for the phase with the given parity; gives up after `limit` cycles
+// (2^32 by default, about 2 s).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = 1ll << 32)
 {
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
-        if (clock64() - t0 > (1ll << 32))
+        if (clock64() - t0 > limit)
             return false;
     }
     return true;
@@ -162,6 +163,20 @@ struct KSw {
 __device__ int g_err;   // first error code seen by a kernel of this file (0: none)
 
 __device__ __forceinline__ void set_err(int code) { atomicCAS(&g_err, 0, code); }
+
+// The conv kernels' bounded wait on a barrier whose phase never completes
+// (its one expected arrival never comes): the wait must give up and report.
+__global__ void k_wait_probe(long long limit)
+{
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(&bar);
+    if (threadIdx.x == 0)
+        mbar_init(b, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait(b, 0, limit))
+        set_err(10);
+    __syncthreads();
+}
 
 __device__ __forceinline__ bool interior(int p, int P, int Hp, int Wp)
 {
@@ -1682,6 +1697,20 @@ int fcab_unet_pack_input(const float *in, int Cs, void *x, int C, int N, int H, 
     const long long n = (long long)N * H * W * (C / 8);
     FCAB_CHECK_VEC(C, n);
     FCAB_EW_LAUNCH(k_pack_input, n, in, Cs, (uint4 *)x, C, N, H, W);
+}
+
+// Runs the conv kernels' bounded mbarrier wait on a barrier that nothing
+// arrives at, with a limit of `limit_cycles` (1 to 2^32): the wait gives up,
+// the kernel records error 10 and returns.
+int fcab_unet_wait_probe(long long limit_cycles, void *stream)
+{
+    if (limit_cycles < 1 || limit_cycles > (1ll << 32))
+        return fail(FCAB_ERR_ARG, "wait_probe: limit out of range");
+    k_wait_probe<<<1, 32, 0, (cudaStream_t)stream>>>(limit_cycles);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+    return FCAB_OK;
 }
 
 // Returns and clears the device error code of the surrogate kernels (0: none).

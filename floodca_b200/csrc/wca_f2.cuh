@@ -1,8 +1,8 @@
 // Two FP32 lanes in one 64-bit register pair, operated on by the sm_100a
 // packed instructions add/sub/mul/fma.rn.f32x2. Each packed instruction
-// rounds both halves exactly as the scalar .rn instruction would (one
-// rounding per operation, no contraction), so a computation written on pairs
-// gives the same bits as the same computation on each half. A packed
+// rounds both halves exactly as the scalar .rn instruction would, so a
+// computation written on pairs gives the same bits as the same computation on
+// each half, provided no packed product feeds a packed sum (see mul2_sep). A packed
 // instruction takes one issue slot for two operations; the FMA pipe still
 // spends a cycle on each half. Comparisons, selects, min/max and the MUFU
 // approximations have no packed form and run per half.
@@ -59,6 +59,15 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b)
     f2 r;
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.u) : "l"(a.u), "l"(b.u));
     return r;
+}
+// RN(a*b) per half, as two scalar products: ptxas (CUDA 12.9) contracts a
+// mul.rn.f32x2 whose result feeds an add.rn.f32x2 or sub.rn.f32x2 into one
+// fused multiply-add, even with --fmad=false, and folds fma.rn.f32x2 with a
+// -0 addend back into that product; scalar mul.rn is never contracted. Use
+// this wherever a product is later summed and both roundings must happen.
+__device__ __forceinline__ f2 mul2_sep(f2 a, f2 b)
+{
+    return mk2(__fmul_rn(lo2(a), lo2(b)), __fmul_rn(hi2(a), hi2(b)));
 }
 // a*b + c with one rounding
 __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
@@ -166,7 +175,7 @@ __device__ __forceinline__ f2 cbrt_sq2(f2 hf, bool &unsure0, bool &unsure1)
 {
     const f2 l = lg2_2(hf);
     const f2 u0 = ex2_2(mul2(l, bc2(0.333333343f)));
-    const f2 s_hi = mul2(u0, u0);
+    const f2 s_hi = mul2_sep(u0, u0);
     const f2 s_lo = fma2(u0, u0, neg2(s_hi));
     const f2 r1 = fma2(s_hi, u0, neg2(hf));
     const f2 r = fma2(s_lo, u0, r1);                        // u0^3 - hf

@@ -82,15 +82,18 @@ __global__ void k_fill_all(void *p, long long n, double v, int esize)
 // so a uniform field can be detected exactly.
 template <typename T>
 __global__ void k_make_cr(const T *C, const T *R, const uint8_t *m, T *cr, long long pitch,
-                          int r_lo, int nr, int nc, unsigned long long *mm)
+                          int r_lo, int nr, int nc, unsigned long long *mm, const T *z,
+                          const T *h, const T *n)
 {
-    unsigned long long lo = ~0ull, hi = 0ull;
+    unsigned long long lo = ~0ull, hi = 0ull, bad = ~0ull;
     const long long N = (long long)nr * nc;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
         const int r = r_lo + (int)(i / nc), c = (int)(i % nc);
         const long long a = (long long)(r + PADR) * pitch + c + PADC;
-        const T v = C[a] * R[a];
+        // rain falls on LAND cells only; other cells keep 0 whatever C and
+        // Rday hold there
+        const T v = m[a] == M_LAND ? C[a] * R[a] : T(0);
         cr[a] = v;
         if (m[a] == M_LAND) {
             unsigned long long key;
@@ -103,10 +106,27 @@ __global__ void k_make_cr(const T *C, const T *R, const uint8_t *m, T *cr, long 
             }
             lo = key < lo ? key : lo;
             hi = key > hi ? key : hi;
+            // first non-finite input of a LAND cell: 8 * cell + field
+            // (0 z, 1 h, 2 n, 3 C, 4 Rday); z, h, n only when given
+            int f = -1;
+            if (z && !isfinite(z[a]))
+                f = 0;
+            else if (z && !isfinite(h[a]))
+                f = 1;
+            else if (z && !isfinite(n[a]))
+                f = 2;
+            else if (!isfinite(C[a]))
+                f = 3;
+            else if (!isfinite(R[a]))
+                f = 4;
+            if (f >= 0 && bad == ~0ull)
+                bad = (unsigned long long)i * 8 + f;
         }
     }
     atomicMin(&mm[0], lo);
     atomicMax(&mm[1], hi);
+    if (bad != ~0ull)
+        atomicMin(&mm[2], bad);
 }
 
 size_t esize_of(int prec) { return prec == FCAB_PREC_F64 ? 8 : 4; }
@@ -277,17 +297,59 @@ long long fcab::step_warps(const FcabConfig &c, int cpl, int nsm, int per_sm, in
     return warps < 1 ? 1 : warps;
 }
 
+// Rejects configurations the step cannot run: unknown enumerations, a dt
+// reuse count below 1, non-positive or non-finite cell size, gravity,
+// Courant factor or dt bounds (a zero dt never advances the clock), negative
+// thresholds, non-finite times and unsupported launch overrides. Makes no
+// CUDA call.
+static int validate_config(const FcabConfig *c)
+{
+    auto pos = [](double v) { return std::isfinite(v) && v > 0.0; };
+    auto nonneg = [](double v) { return std::isfinite(v) && v >= 0.0; };
+    if (c->nrows < 1 || c->ncols < 1)
+        return fail(FCAB_ERR_ARG, "grid %dx%d is empty", c->nrows, c->ncols);
+    if ((long long)c->nrows * c->ncols > (1ll << 40))
+        return fail(FCAB_ERR_ARG, "grid too large");
+    if (c->K != 4 && c->K != 8)
+        return fail(FCAB_ERR_ARG, "K=%d: only 4 or 8 neighbours", c->K);
+    if (c->precision < FCAB_PREC_F32 || c->precision > FCAB_PREC_F64)
+        return fail(FCAB_ERR_ARG, "unknown precision %d", c->precision);
+    if (c->math != FCAB_MATH_EXACT && c->math != FCAB_MATH_FAST)
+        return fail(FCAB_ERR_ARG, "unknown math mode %d", c->math);
+    if (c->U < 1)
+        return fail(FCAB_ERR_ARG, "U=%d: the dt reuse count is at least 1", c->U);
+    if (c->boundary != FCA_BND_OPEN && c->boundary != FCA_BND_CLOSED)
+        return fail(FCAB_ERR_ARG, "unknown boundary %d", c->boundary);
+    if (c->hyeto != FCA_HYETO_TRIANGLE && c->hyeto != FCA_HYETO_UNIFORM)
+        return fail(FCAB_ERR_ARG, "unknown hyetograph %d", c->hyeto);
+    if (!pos(c->dx) || !pos(c->g) || !pos(c->alpha))
+        return fail(FCAB_ERR_ARG, "dx, g and alpha must be finite and positive");
+    if (!pos(c->dt_max) || !pos(c->dt_min))
+        return fail(FCAB_ERR_ARG, "dt_max and dt_min must be finite and positive");
+    if (!nonneg(c->tau_h) || !nonneg(c->tau_l))
+        return fail(FCAB_ERR_ARG, "tau_h and tau_l must be finite and not negative");
+    if (!std::isfinite(c->z_sea) || !std::isfinite(c->S_bnd) || !std::isfinite(c->T_sim) ||
+        !std::isfinite(c->out_every) || !std::isfinite(c->D_h) || !std::isfinite(c->phi) ||
+        !std::isfinite(c->rain_end))
+        return fail(FCAB_ERR_ARG, "z_sea, S_bnd, T_sim, out_every, D_h, phi and rain_end must be finite");
+    if (c->max_steps < 0)
+        return fail(FCAB_ERR_ARG, "max_steps=%d is negative", c->max_steps);
+    if (c->cols_per_lane != 0 && c->cols_per_lane != 1 && c->cols_per_lane != 2 &&
+        c->cols_per_lane != 4)
+        return fail(FCAB_ERR_ARG, "cols_per_lane=%d: 0, 1, 2 or 4", c->cols_per_lane);
+    if (c->seg_rows < 0)
+        return fail(FCAB_ERR_ARG, "seg_rows=%d is negative", c->seg_rows);
+    if (c->inflow_cell >= 0 && (!std::isfinite(c->inflow_peak) || !std::isfinite(c->inflow_t_peak) ||
+                                !std::isfinite(c->inflow_t_end)))
+        return fail(FCAB_ERR_ARG, "inflow hydrograph values must be finite");
+    return FCAB_OK;
+}
+
 extern "C" int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *stream)
 {
     *out = nullptr;
-    if (cfg->nrows < 1 || cfg->ncols < 1)
-        return fail(FCAB_ERR_ARG, "grid %dx%d is empty", cfg->nrows, cfg->ncols);
-    if (cfg->K != 4 && cfg->K != 8)
-        return fail(FCAB_ERR_ARG, "K=%d: only 4 or 8 neighbours", cfg->K);
-    if (cfg->precision < FCAB_PREC_F32 || cfg->precision > FCAB_PREC_F64)
-        return fail(FCAB_ERR_ARG, "unknown precision %d", cfg->precision);
-    if ((long long)cfg->nrows * cfg->ncols > (1ll << 40))
-        return fail(FCAB_ERR_ARG, "grid too large");
+    if (int rc = validate_config(cfg))
+        return rc;
 
     FcabSim *s = new FcabSim();
     s->cfg = *cfg;
@@ -412,10 +474,12 @@ static int fill_interior(FcabSim *s, void *dst, double v)
 }
 
 // Rebuilds cr = C*Rday from the staging copies tmpC/tmpR (padded layout)
-// and decides whether the field is uniform over LAND cells.
-static int rebuild_rain(FcabSim *s)
+// and decides whether the field is uniform over LAND cells. Fails with
+// FCAB_ERR_ARG when a LAND cell's C or Rday (and, with check_state, its z,
+// h or n) is not finite.
+static int rebuild_rain(FcabSim *s, bool check_state)
 {
-    unsigned long long init[2] = {~0ull, 0ull};
+    unsigned long long init[3] = {~0ull, 0ull, ~0ull};
     CUDA_TRY(cudaMemcpyAsync(s->scratch, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
     if (!s->cr)
         CUDA_TRY(fcab::cached_malloc(&s->cr, s->nelem * s->esize));
@@ -424,15 +488,25 @@ static int rebuild_rain(FcabSim *s)
     if (s->esize == 8)
         k_make_cr<double><<<nb, 256, 0, s->stream>>>(
             (const double *)s->tmpC, (const double *)s->tmpR, s->m, (double *)s->cr, s->pitch,
-            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch);
+            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch,
+            check_state ? (const double *)s->z : nullptr, (const double *)s->h0,
+            (const double *)s->n);
     else
         k_make_cr<float><<<nb, 256, 0, s->stream>>>(
             (const float *)s->tmpC, (const float *)s->tmpR, s->m, (float *)s->cr, s->pitch,
-            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch);
+            -s->hn, s->cfg.nrows + s->hn + s->hs, s->cfg.ncols, (unsigned long long *)s->scratch,
+            check_state ? (const float *)s->z : nullptr, (const float *)s->h0,
+            (const float *)s->n);
     CUDA_TRY(cudaGetLastError());
-    unsigned long long mm[2];
+    unsigned long long mm[3];
     CUDA_TRY(cudaMemcpyAsync(mm, s->scratch, sizeof(mm), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (mm[2] != ~0ull) {
+        static const char *names[5] = {"z", "h", "n", "C", "Rday"};
+        const long long cell = (long long)(mm[2] >> 3);
+        return fail(FCAB_ERR_ARG, "%s is not finite at LAND cell (row %lld, col %lld)",
+                    names[mm[2] & 7], cell / s->cfg.ncols - s->hn, cell % s->cfg.ncols);
+    }
     double uni = 0.0;
     bool uniform = true;
     if (mm[0] != ~0ull) {
@@ -499,7 +573,7 @@ static int upload_common(FcabSim *s, const void *z, const void *h, const void *n
         CUDA_TRY(put_field(s, s->tmpC, C, es, kind));
     if (Rday)
         CUDA_TRY(put_field(s, s->tmpR, Rday, es, kind));
-    int rc = rebuild_rain(s);
+    int rc = rebuild_rain(s, true);
     if (rc)
         return rc;
     // has SEA / inflow cell LAND
@@ -584,7 +658,7 @@ extern "C" int fcab_sim_set_rain(FcabSim *s, const void *C, const void *Rday)
         CUDA_TRY(put_field(s, s->tmpC, C, s->esize, cudaMemcpyHostToDevice));
     if (Rday)
         CUDA_TRY(put_field(s, s->tmpR, Rday, s->esize, cudaMemcpyHostToDevice));
-    return rebuild_rain(s);
+    return rebuild_rain(s, false);
 }
 
 static int resolve_variant(FcabSim *s)
@@ -961,6 +1035,8 @@ extern "C" int fcab_sim_set_config(FcabSim *s, const FcabConfig *cfg)
     if (cfg->nrows != o.nrows || cfg->ncols != o.ncols || cfg->precision != o.precision ||
         cfg->K != o.K)
         return fail(FCAB_ERR_ARG, "set_config cannot change the grid, precision or K");
+    if (int rc = validate_config(cfg))
+        return rc;
     const int keep_cpl = s->cpl;
     const int has_sea = s->esize == 8 ? s->rkd.has_sea : s->rkf.has_sea;
     const double cru = s->esize == 8 ? s->rkd.cr_uniform : (double)s->rkf.cr_uniform;
@@ -1268,8 +1344,9 @@ __global__ void k_math_probe(int which, const float *x, const float *y, float *o
             const f2 c = cbrt_sq2(mk2(x[i], x[i]), u0, u1);
             r = u0 ? __int_as_float(0x7fc00000) : lo2(c);
         } else if (which == 11) {
-            // a packed product then a packed sum: two roundings, RN(RN(x*y) + g)
-            r = lo2(add2(mul2(mk2(x[i], x[i]), mk2(y[i], y[i])), bc2(g)));
+            // the pair sweep's product then packed sum: two roundings,
+            // RN(RN(x*y) + g)
+            r = lo2(add2(mul2_sep(mk2(x[i], x[i]), mk2(y[i], y[i])), bc2(g)));
         } else
             r = __fdiv_rn(x[i], y[i]);
         out[i] = r;

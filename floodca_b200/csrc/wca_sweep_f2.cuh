@@ -569,13 +569,13 @@ struct PairSweep {
             }
             f2 rain = c.rain;
             if constexpr (RAINF)
-                rain = mul2(R.cr[Sm2], bc2(sv.F));
+                rain = mul2_sep(R.cr[Sm2], bc2(sv.F));
             f2 dq;
             if constexpr (MATH == MATH_EXACT)
                 dq = div2_mk(net, c.A, c.invA);
             else
                 dq = mul2(net, c.invA);
-            f2 hu = add2(R.h[Sm2], add2(mul2(c.dt, dq), rain));
+            f2 hu = add2(R.h[Sm2], add2(mul2_sep(c.dt, dq), rain));
             {
                 float u0, u1;
                 sp2(hu, u0, u1);

@@ -102,6 +102,7 @@ def core() -> C.CDLL:
                                      C.c_float, _I, C.c_float, _P]),
         "fcab_unet_pack_input": (C.c_int, [_P, _I, _P, _I, _I, _I, _I, _P]),
         "fcab_unet_device_error": (C.c_int, []),
+        "fcab_unet_wait_probe": (C.c_int, [_LL, _P]),
         "fcab_last_error": (C.c_char_p, []),
         "fcab_version": (C.c_char_p, []),
     }

@@ -396,8 +396,8 @@ FCAB_API int fcab_run_noalloc(const FcabConfig *cfg, const float *z, const float
  * hf^(2/3); 1: min(x, RN(sqrt(g*y))); 2: the fast-mode hf^(2/3); 4/5/6: the
  * branch-free reciprocal, square root and Markstein quotient x/y; 7/8/9: the
  * IEEE reciprocal, square root and quotient they must equal; 10: the packed
- * pair sweep's hf^(2/3), NaN where it defers to the exact evaluation; 11: a
- * packed product then a packed sum, RN(RN(x*y) + g), rounded twice. */
+ * pair sweep's hf^(2/3), NaN where it defers to the exact evaluation; 11: the
+ * pair sweep's product then packed sum, RN(RN(x*y) + g), rounded twice. */
 FCAB_API int fcab_math_probe(int which, const float *x, const float *y, float *out, long long n,
                              float g);
 
@@ -494,6 +494,10 @@ FCAB_API int fcab_unet_pack_input(const float *in, int Cs, void *x, int C, int N
 /* Returns and clears the device-side error code of these kernels (0: none;
  * nonzero: a pipeline wait gave up). */
 FCAB_API int fcab_unet_device_error(void);
+/* Failure-path probe: runs the kernels' bounded mbarrier wait on a barrier
+ * that nothing completes, giving up after limit_cycles (1 to 2^32) SM
+ * cycles; fcab_unet_device_error() then returns 10. */
+FCAB_API int fcab_unet_wait_probe(long long limit_cycles, void *stream);
 
 #ifdef __cplusplus
 }

@@ -131,8 +131,11 @@ def test_packed_cube_root_decides_only_correct_roundings():
 
 
 def test_packed_product_then_sum_rounds_twice():
-    """A packed multiply feeding a packed add must not be contracted into a
-    fused multiply-add (the reference rounds the product, then the sum)."""
+    """The pair sweep's product feeding a packed add must not be contracted
+    into a fused multiply-add (the reference rounds the product, then the
+    sum). ptxas contracts a mul.rn.f32x2 feeding an add.rn.f32x2 even with
+    --fmad=false, so the sweep forms such products as two scalar mul.rn
+    (mul2_sep); this checks that form on the device."""
     from floodca_b200.lib import core
     rng = np.random.default_rng(10)
     x = rng.uniform(0.5, 2.0, 1_000_000).astype(np.float32)

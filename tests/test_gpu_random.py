@@ -8,8 +8,8 @@ Each grid also runs as an all-LAND grid (SEA and WALL cells turned to LAND),
 which takes the all-LAND kernels, with the random C*Rday field as a per-cell
 rain field. Both lane widths run: one column per lane and two (the packed
 pair sweep on all-LAND grids). FP32 must equal the reference bit for bit;
-FP64 within 1e-12 m (the device's and glibc's double cube roots may differ in
-the last bit)."""
+FP64 depths within 1e-12 m and times within 1e-9 s (the device's and glibc's
+double cube roots may differ in the last bit)."""
 import numpy as np
 import pytest
 
@@ -32,7 +32,10 @@ def _check(r, ref, kind):
         if kind == "f32":
             assert np.array_equal(r[k], ref[k]), k
         else:
-            assert np.abs(np.asarray(r[k], np.float64) - ref[k]).max() <= 1e-12, k
+            # depths within 1e-12 m; tmax holds times (seconds), which carry
+            # the clock's last-bit differences, within the same 1e-9 s as t
+            tol = 1e-9 if k == "tmax" else 1e-12
+            assert np.abs(np.asarray(r[k], np.float64) - ref[k]).max() <= tol, k
     for k in ("V_rain", "V_sea", "V_bnd", "clamp_err"):
         assert r[k] == pytest.approx(ref[k], rel=1e-9, abs=1e-6), k
     assert r["cap_active"] == ref["cap_active"]

@@ -337,3 +337,34 @@ def test_fused_upcat_and_pool_backward_add():
     want = _from_b(plain, N, H, W)[:, 1:-1, 1:-1] + g[..., C1:]
     assert np.allclose(_from_b(fused, N, H, W)[:, 1:-1, 1:-1], want, rtol=8e-3, atol=1e-2)
     assert _border_zero(fused, N, H, W) and _border_zero(cat, N, H, W)
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """The conv kernels' mbarrier wait on a phase that never completes (no
+    arrival ever comes) gives up after its limit, records error 10 and
+    returns; the context stays usable and a following convolution is
+    correct with no error recorded."""
+    L = core()
+    assert L.fcab_unet_device_error() == 0
+    assert L.fcab_unet_wait_probe(0, None) != 0                 # limit out of range
+    assert L.fcab_unet_wait_probe(1 << 20, None) == 0           # about half a millisecond
+    torch.cuda.synchronize()
+    assert L.fcab_unet_device_error() == 10
+    assert L.fcab_unet_device_error() == 0                      # read clears it
+    N, H, W, Cin, Cout = 1, 8, 8, 16, 32
+    rng = np.random.default_rng(4)
+    x = _bf(rng.standard_normal((N, H, W, Cin)))
+    w = _bf(rng.standard_normal((Cout, 9, Cin)) / 12.0)
+    xb = _to_b(x)
+    wf = torch.tensor(w).cuda()
+    wb = torch.empty((Cout, 9, Cin), dtype=torch.bfloat16, device="cuda")
+    wt = torch.empty((Cin, 9, Cout), dtype=torch.bfloat16, device="cuda")
+    L.fcab_unet_prep_weights(_p(wf), _p(wb), _p(wt), Cout, Cin, None)
+    y = torch.zeros((xb.shape[0], Cout), dtype=torch.bfloat16, device="cuda")
+    assert L.fcab_unet_conv_fwd(_p(xb), N, H, W, Cin, _p(wb), Cout, None, 0, _p(y), None) == 0
+    torch.cuda.synchronize()
+    assert L.fcab_unet_device_error() == 0
+    xt = torch.tensor(x).permute(0, 3, 1, 2)
+    wt4 = torch.tensor(w).view(Cout, 3, 3, Cin).permute(0, 3, 1, 2)
+    yr = torch.nn.functional.conv2d(xt, wt4, padding=1).permute(0, 2, 3, 1).numpy()
+    assert _close(_from_b(y, N, H, W)[:, 1:H + 1, 1:W + 1], yr, 8e-3) <= 1.0

@@ -1,7 +1,10 @@
 """Batched ensembles (fcab_batch_*): every member of a batch ends with the
 same depth, max depth, time of max depth, step count and simulated time as
 the same member run alone in its own session, bit for bit, whatever the mix
-of member sizes, parameters and rain; output windows only pace the members."""
+of member sizes, parameters and rain; output windows only pace the members.
+Each member of the mixed batches is also compared with the compiled
+reference core run on its own (FP32 bit for bit), the semantics the batch
+replaces being one fca_cuda_ens_run per member (src/cuda/kernels.cu:836-997)."""
 import ctypes as C
 
 import numpy as np
@@ -11,6 +14,7 @@ from floodca_b200 import abi, synth
 from floodca_b200.ensemble import Batch, Member, member_session
 from floodca_b200.lib import FcabError
 from floodca_b200.sim import Session, run_session
+from tests import refpin
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +37,11 @@ def _members(K=4, rain_field=False, sea=False, seed=11):
             d.mask[:, :1] = abi.FCA_WALL
         out.append((d, p))
     return out
+
+
+def _result(s):
+    h, hmax, tmax = s.download()
+    return {**s.stats(), "h": h, "hmax": hmax, "tmax": tmax}
 
 
 def _check_equal(single, s):
@@ -58,8 +67,9 @@ def test_batch_equals_single_sessions(K, rain_field, sea, cpl, seg):
         b.run(window=600.0, graph_steps=8)
         info = b.info()
         assert info["members"] == len(mem) and info["windows"] >= 2
-        for single, s in zip(singles, sessions):
+        for single, s, (d, p) in zip(singles, sessions, mem):
             _check_equal(single, s)
+            refpin.check_reference(_result(s), d, p)
     finally:
         b.close()
         for s in sessions:
@@ -96,8 +106,9 @@ def test_batch_free_running():
     try:
         b.run(window=0.0, graph_steps=32)
         assert b.info()["windows"] == 0
-        for single, s in zip(singles, sessions):
+        for single, s, (d, p) in zip(singles, sessions, mem):
             _check_equal(single, s)
+            refpin.check_reference(_result(s), d, p)
     finally:
         b.close()
         for s in sessions:
@@ -130,6 +141,7 @@ def test_device_members_equal_host_members():
     try:
         s.run()
         _check_equal(single, s)
+        refpin.check_reference(_result(s), d, p)
     finally:
         s.close()
 

@@ -1,6 +1,9 @@
 """The reference-facing ensemble session (fca_cuda_ens_*, FloodCA
 src/cuda/kernels.cu:790-1043): each scenario run equals a plain run of the
-same scenario, and the uint16 count rasters add hmax >= thr on LAND cells."""
+same scenario and the compiled reference core's run of it (steps, time,
+volumes), and the flooded-cell counts, the maximum depth and the uint16
+count rasters are those of the reference core's hmax (hmax >= thr on LAND
+cells, as k_ens_count does, src/cuda/kernels.cu:799-823)."""
 import ctypes as C
 
 import numpy as np
@@ -10,6 +13,7 @@ from conftest import GOLDEN
 from floodca_b200 import abi
 from floodca_b200.lib import dropin
 from floodca_b200.sim import DropinGrid
+from tests import refpin
 from tests.golden.make_golden import load_case
 
 pytestmark = pytest.mark.gpu
@@ -41,8 +45,13 @@ def test_ensemble_session_matches_single_runs(double):
             assert g.acc.step == r["step"] and g.acc.t == r["t"]
             assert g.acc.V == pytest.approx(r["V"], rel=1e-12)
             assert g.acc.V_rain == pytest.approx(r["V_rain"], rel=1e-12)
+            kind = "f64" if double else "f32"
+            ref = refpin.reference(ds, p, kind)
+            refpin.check(r, ref, kind, volumes=("V", "V_rain", "V_sea", "V_bnd", "clamp_err"))
+            assert g.acc.step == ref["step"]
+            assert g.acc.V_rain == pytest.approx(ref["V_rain"], rel=1e-9)
             land = ds.mask == abi.FCA_LAND
-            hm = np.asarray(r["hmax"], np.float64)
+            hm = np.asarray(ref["hmax"], np.float64)
             for j, t in enumerate((0.10, 0.25, 0.50)):
                 hit = land & (hm >= t)
                 assert fl[j] == int(hit.sum())

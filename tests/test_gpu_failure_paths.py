@@ -84,7 +84,7 @@ def test_failed_forcing_day_ends_the_run_like_the_reference(how):
 @pytest.mark.parametrize("value", [np.nan, np.inf])
 def test_non_finite_land_input_is_rejected(field, value):
     d, p, f, _ = load_case(GOLDEN / "mixed_k4.npz")
-    g = DropinGrid(d, p)
+    g = DropinGrid(d.copy(), p)          # the grid may share the domain's arrays
     land = np.flatnonzero(d.mask.ravel() == abi.FCA_LAND)
     cell = int(land[len(land) // 2])
     g.arrays[field].reshape(-1)[cell] = value
@@ -109,7 +109,7 @@ def test_non_finite_values_off_land_are_ignored():
     off = np.flatnonzero(m != abi.FCA_LAND)
     sea = np.flatnonzero(m == abi.FCA_SEA)
     assert off.size > 0 and sea.size > 0
-    g = DropinGrid(d, p)
+    g = DropinGrid(d.copy(), p)
     for k in ("n", "C", "Rday"):
         g.arrays[k].reshape(-1)[off] = np.nan
     for k in ("z", "h"):

@@ -4,7 +4,8 @@ depth, step count and time as the same domain run whole, bit for bit, with
 the volumes summed over slabs within rounding. The slabs run on one GPU,
 in one process (device max and device copies between slabs) or in two
 processes that exchange through gloo on the host; no kernel waits on
-another."""
+another. The split runs are also compared with the compiled reference core
+run on the whole domain (FP32 bit for bit, FP64 within 1e-12 m)."""
 import multiprocessing as mp
 import socket
 
@@ -15,6 +16,7 @@ from floodca_b200 import abi, synth
 from floodca_b200.lib import FcabError
 from floodca_b200.sim import run_session
 from floodca_b200.slabs import HALO, Slab, run_split_local, slab_specs
+from tests import refpin
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +69,7 @@ def test_split_equals_whole_domain(parts, kw):
     single = run_session(d, p)
     split = run_split_local(d, p, parts)
     _check_equal(single, split)
+    refpin.check_reference(split, d, p)
 
 
 @pytest.mark.parametrize("K", [4, 8])
@@ -84,7 +87,9 @@ def test_split_deferred_dt(K):
     p = p.with_(T_sim=900.0)
     single = run_session(d, p)
     assert single["dt_full_passes"] > 0
-    _check_equal(single, run_split_local(d, p, 3))      # slab edges at rows 30 and 60
+    split = run_split_local(d, p, 3)                    # slab edges at rows 30 and 60
+    _check_equal(single, split)
+    refpin.check_reference(split, d, p)
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32all"])
@@ -94,6 +99,8 @@ def test_split_precisions(precision):
     split = run_split_local(d, p, 2, precision=precision)
     # f32all accumulates the volumes in float
     _check_equal(single, split, rel=1e-5 if precision == "f32all" else 1e-11)
+    if precision == "f64":
+        refpin.check_reference(split, d, p, kind="f64")
 
 
 def test_split_cols_per_lane_and_segments():
@@ -101,9 +108,11 @@ def test_split_cols_per_lane_and_segments():
     segments) give the same results."""
     d, p = _domain(200, 300, K=4, inflow_row=99)
     single = run_session(d, p)
+    ref = refpin.reference(d, p)
     for cpl, seg in ((1, 8), (4, 64)):
         split = run_split_local(d, p, 2, cols_per_lane=cpl, seg_rows=seg)
         _check_equal(single, split)
+        refpin.check(split, ref)
 
 
 def test_rows_round_trip_and_bounds():
@@ -179,3 +188,4 @@ def test_rank_slabs_two_processes_gloo():
         pr.join(timeout=120)
         assert pr.exitcode == 0
     _check_equal(single, out)
+    refpin.check_reference(out, d, p)

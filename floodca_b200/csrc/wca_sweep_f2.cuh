@@ -10,14 +10,16 @@
 //    multiply and fused multiply-add runs on both columns in one instruction
 //    (the same rounding per half as the scalar instruction);
 //  * the pipeline's rows live in a four-slot register ring (row r in slot
-//    (r - i0) & 3 of an unrolled pass, or rotated one slot per row);
-//  * the exact formulas run optimistically: each face takes the common path
-//    (no critical-velocity cap, no volume cap, a cube root whose rounding is
-//    decided) and flags the halves where that is not certain; a warp with a
-//    flagged half re-evaluates those halves with the exact scalar formula
-//    (face_q). The same holds for the limiter (a division only where the
-//    outflow exceeds the held volume), the clamp and the next-step velocity
-//    (a multiply-only bound h^4 S^3 >= thr^6 n^6 before the exact value);
+//    (r - i0) & 3 of a four-row pass, turned by two slots after a two-row
+//    pass, or rotated one slot per row);
+//  * the exact formulas run on pairs with correctly rounded divisions, roots
+//    and caps (the volume cap by a Markstein division, the critical velocity
+//    from the exact product g*hf when a warp has a face near it); a cube root
+//    or critical velocity within 2^-11 ulp of a rounding midpoint flags its
+//    half, and a warp with a flagged half re-evaluates those halves with the
+//    exact scalar formula (face_q). The limiter divides only where the
+//    outflow exceeds the held volume, and the next-step velocity first tests
+//    a multiply-only bound h^4 S^3 >= thr^6 n^6;
 //  * the upwind-scaled discharge of every face is formed once, as
 //    Q- * s_down + Q+ * s_up with Q+ = max(Q, 0), Q- = min(Q, 0) (one of the
 //    two products is zero, so this is the reference's Q * s_upwind), and
@@ -38,10 +40,11 @@ namespace fcab {
 constexpr int TMA_RB = 8, TMA_NS = 3;
 
 // Iterations per pass of the pair sweep's loop: 4 unrolls the body over the
-// four ring slots (no register copies, four copies of the code); 1 runs one
-// body and rotates the ring's registers after each row. Measured at 4096^2
-// on a B200: the one-row loop is faster (33.9 against 18.9 Gcell/s at 12
-// warps per SM): the unrolled body misses the instruction cache.
+// four ring slots (no register copies, four copies of the code); 2 runs two
+// bodies and turns the ring by two slots after them; 1 runs one body and
+// rotates the ring's registers after each row. Measured at 4096^2 on a
+// B200: the one-row loop is faster than four (33.9 against 18.9 Gcell/s at
+// 12 warps per SM): the four-row body misses the instruction cache.
 #ifndef FCAB_PAIR_UNROLL
 #define FCAB_PAIR_UNROLL 1
 #endif
@@ -58,7 +61,8 @@ __host__ __device__ constexpr int tma_smem_bytes(int warps)
 
 // Packed per-step constants of the pair sweep.
 struct PairK {
-    f2 dx, rdx, dd, rdd, w, A, invA, g, dt, rain, half, nmin, vcrK, capK;
+    f2 dx, rdx, dd, rdd, w, A, invA, g, dt, rain, half, nmin, vcrK;
+    f2 den, rden;                       // 2K dt and RN(1/(2K dt)) (volume cap)
     float tau_l, tau_h;
 };
 
@@ -83,17 +87,48 @@ __device__ __forceinline__ f2 lds2(uint32_t a)
     return mk2(x, y);
 }
 
+// RN(sqrt(g*hf)) per half of the exact product g*hf (as the reference's
+// (real)sqrt((double)g*(double)hf), physics.h:107-108): from p = RN(g*hf),
+// its error pe = g*hf - p (exact, one fused multiply-add) and s = RN(sqrt(p)),
+// the root of p + pe is s + (p - s^2 + pe)/(2s) to far better than 2^-20 ulp;
+// that sum is rounded to y with its error e (Fast2Sum). `unsure` per half:
+// |e| within 2^-11 of half an ulp of y (tested as fma(e, 1 + 2^-11, y) != y),
+// which also covers the reference's double rounding (its root is rounded to
+// double first, which can only matter within 2^-29 ulp of a midpoint). The
+// exact value is never a float midpoint: a midpoint has 25 significant bits,
+// its square at least 49, and g*hf at most 48.
+__device__ __forceinline__ f2 vcrit2(f2 g, f2 hf, bool &unsure0, bool &unsure1)
+{
+    const f2 p = mul2(g, hf);
+    const f2 pe = fma2(g, hf, neg2(p));
+    const f2 y0 = rsqrt_2(p);
+    const f2 s0 = mul2(p, y0);
+    const f2 h = mul2(bc2(0.5f), y0);
+    const f2 s = fma2(fma2(neg2(s0), s0, p), h, s0);       // RN(sqrt(p))
+    const f2 r = add2(fma2(neg2(s), s, p), pe);              // g*hf - s^2
+    const f2 corr = mul2_sep(r, h);
+    const f2 y = add2(s, corr);
+    const f2 e = add2(sub2(s, y), corr);
+    const f2 chk = fma2(e, bc2(1.00048828125f), y);
+    float y0f, y1f, k0, k1;
+    sp2(y, y0f, y1f);
+    sp2(chk, k0, k1);
+    unsure0 = k0 != y0f;
+    unsure1 = k1 != y1f;
+    return y;
+}
+
 // Discharge a -> b of two faces (one per half) between all-LAND cells with
 // old levels La, Lb, elevations za, zb and Manning n na, nb, centre distance
-// d (rd = RN(1/d)) and width w (FloodCA src/kernels/physics.h:51-125).
-// MATH_EXACT: the common path; `un0`/`un1` flag live halves whose value the
-// exact scalar formula must settle (cube root near a rounding midpoint or
-// out of range, velocity near or above the critical velocity, volume cap
-// possibly binding). MATH_FAST: hardware approximations throughout, volume
-// cap applied; `un*` then flag capped halves (for the cap count).
+// d (rd = RN(1/d)) and width w (FloodCA src/kernels/physics.h:51-125), with
+// the critical-velocity and volume caps. `cap0`/`cap1`: live halves whose
+// volume cap binds. MATH_EXACT: every operation rounded as the reference's;
+// `un0`/`un1` flag live halves whose value the exact scalar formula must
+// settle (a cube root or critical velocity near a rounding midpoint, or out
+// of range). MATH_FAST: hardware approximations throughout; no flags.
 template <int MATH>
 __device__ __forceinline__ f2 face2(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2 d, f2 rd, f2 w,
-                                    const PairK &c, bool &un0, bool &un1)
+                                    const PairK &c, bool &un0, bool &un1, bool &cap0, bool &cap1)
 {
     const f2 dL = sub2(La, Lb);
     const f2 Lmx = max2(La, Lb);
@@ -105,24 +140,29 @@ __device__ __forceinline__ f2 face2(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2
     const bool live0 = a0 >= c.tau_l && h0 >= c.tau_h;
     const bool live1 = a1 >= c.tau_l && h1 >= c.tau_h;
     const f2 nf = max2(mul2(c.half, add2(na, nb)), c.nmin);
-    f2 Qm;
+    f2 Qm, Qc;
     if constexpr (MATH == MATH_EXACT) {
         const f2 rnf = rcp2_nr(nf);
         const f2 sq = sqrt2_nr(div2_mk(adL, d, rd));
         bool s0, s1;
         const f2 cb = cbrt_sq2(hf, s0, s1);
-        const f2 v = mul2(mul2(rnf, cb), sq);
+        f2 v = mul2(mul2(rnf, cb), sq);
+        // v^2 < g hf (1 - 1e-6) leaves v surely below the critical velocity
         const f2 v2 = mul2(v, v);
         const f2 pm = mul2(mul2(c.g, hf), c.vcrK);
+        const bool cr0 = live0 && !(lo2(v2) < lo2(pm));
+        const bool cr1 = live1 && !(hi2(v2) < hi2(pm));
+        bool vu0 = false, vu1 = false;
+        if (__any_sync(0xffffffffu, cr0 || cr1)) {
+            const f2 vcr = vcrit2(c.g, hf, vu0, vu1);
+            v = sel2(cr0, cr1, min2(v, vcr), v);
+            vu0 = cr0 && vu0;
+            vu1 = cr1 && vu1;
+        }
         Qm = mul2(mul2(v, hf), w);
-        const f2 qc = mul2(adL, c.capK);             // below the exact volume cap
-        float v20, v21, p0, p1, q0, q1, m0, m1;
-        sp2(v2, v20, v21);
-        sp2(pm, p0, p1);
-        sp2(qc, q0, q1);
-        sp2(Qm, m0, m1);
-        un0 = live0 && (s0 || !(v20 < p0) || !(q0 > m0));
-        un1 = live1 && (s1 || !(v21 < p1) || !(q1 > m1));
+        Qc = div2_mk(mul2(adL, c.A), c.den, c.rden);    // RN(RN(|dL| A) / (2K dt))
+        un0 = live0 && (s0 || vu0);
+        un1 = live1 && (s1 || vu1);
     } else {
         const f2 rnf = rcp_2(nf);
         const f2 S = mul2(adL, rd);
@@ -134,13 +174,12 @@ __device__ __forceinline__ f2 face2(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2
         const f2 v2 = mul2(v, v);
         v = sel2(lo2(v2) > lo2(p), hi2(v2) > hi2(p), vcr, v);
         Qm = mul2(mul2(v, hf), w);
-        const f2 Qc = mul2(mul2(adL, c.A), c.capK);
-        const bool c0 = lo2(Qc) < lo2(Qm), c1 = hi2(Qc) < hi2(Qm);
-        Qm = sel2(c0, c1, Qc, Qm);
-        un0 = live0 && c0;
-        un1 = live1 && c1;
+        Qc = mul2(mul2(adL, c.A), c.rden);
+        un0 = un1 = false;
     }
-    const f2 Q = copysign2(Qm, dL);
+    cap0 = live0 && lo2(Qc) < lo2(Qm);
+    cap1 = live1 && hi2(Qc) < hi2(Qm);
+    const f2 Q = copysign2(min2(Qm, Qc), dL);
     return sel2(live0, live1, Q, bc2(0.0f));
 }
 
@@ -284,6 +323,30 @@ __device__ __forceinline__ void rot4(V (&a)[4])
     a[2] = a[3];
     a[3] = t;
 }
+// The ring viewed two rows further: slots q and q+2 swap.
+template <typename V>
+__device__ __forceinline__ void rot4x2(V (&a)[4])
+{
+    V t = a[0];
+    a[0] = a[2];
+    a[2] = t;
+    t = a[1];
+    a[1] = a[3];
+    a[3] = t;
+}
+template <int K>
+__device__ __forceinline__ void rotate_ring2(PairRing<K> &R)
+{
+    rot4x2(R.z); rot4x2(R.h); rot4x2(R.n); rot4x2(R.L);
+    rot4x2(R.X); rot4x2(R.Y);
+    rot4x2(R.s); rot4x2(R.Qy); rot4x2(R.hn); rot4x2(R.Ln); rot4x2(R.n6);
+    rot4x2(R.hm); rot4x2(R.cr); rot4x2(R.qo); rot4x2(R.ko); rot4x2(R.ef);
+    if constexpr (K == 8) {
+        rot4x2(R.zr); rot4x2(R.hr); rot4x2(R.nr); rot4x2(R.Lr);
+        rot4x2(R.E); rot4x2(R.W);
+        rot4x2(R.Qe); rot4x2(R.Qw);
+    }
+}
 template <int K>
 __device__ __forceinline__ void rotate_ring(PairRing<K> &R)
 {
@@ -368,9 +431,10 @@ struct PairSweep {
             G.o1 += pitch;
             if constexpr (TMA) {
                 // row i+1 is row i+1-i0 of the stream: a new block every 8
-                // rows, which (8 being a multiple of 4) an unrolled pass
-                // only meets at J = 3
-                if ((FCAB_PAIR_UNROLL == 1 || J == 3) && ((i + 1 - G.i0) & (TMA_RB - 1)) == 0)
+                // rows, which (8 being a multiple of the rows per pass) a
+                // pass only meets in its last iteration
+                if ((FCAB_PAIR_UNROLL == 1 || J == FCAB_PAIR_UNROLL - 1) &&
+                    ((i + 1 - G.i0) & (TMA_RB - 1)) == 0)
                     tma_turn(G, lane);
                 R.z[S1] = lds2(G.srow);
                 R.h[S1] = lds2(G.srow + TMA_FIELD_B);
@@ -399,26 +463,36 @@ struct PairSweep {
         {
             R.L[S0] = add2(R.z[S0], R.h[S0]);
             const f2 zr = right2(R.z[S0]), Lr = right2(R.L[S0]), nrr = right2(R.n[S0]);
-            bool ux0, ux1, uy0, uy1;
+            bool ux0, ux1, uy0, uy1, cx0, cx1, cy0, cy1;
             f2 X = face2<MATH>(R.L[S0], Lr, R.z[S0], zr, R.n[S0], nrr, c.dx, c.rdx, c.w, c,
-                               ux0, ux1);
+                               ux0, ux1, cx0, cx1);
             f2 Y = face2<MATH>(R.L[Sm1], R.L[S0], R.z[Sm1], R.z[S0], R.n[Sm1], R.n[S0], c.dx, c.rdx,
-                               c.w, c, uy0, uy1);
+                               c.w, c, uy0, uy1, cy0, cy1);
             f2 E = z0, W = z0;
             bool ue0 = false, ue1 = false, uw0 = false, uw1 = false;
+            bool ce0 = false, ce1 = false, cw0 = false, cw1 = false;
             if constexpr (K == 8) {
                 R.zr[S0] = zr;
                 R.Lr[S0] = Lr;
                 R.nr[S0] = nrr;
                 E = face2<MATH>(R.L[Sm1], Lr, R.z[Sm1], zr, R.n[Sm1], nrr, c.dd, c.rdd, c.w, c, ue0,
-                                ue1);
+                                ue1, ce0, ce1);
                 W = face2<MATH>(R.Lr[Sm1], R.L[S0], R.zr[Sm1], R.z[S0], R.nr[Sm1], R.n[S0], c.dd,
-                                c.rdd, c.w, c, uw0, uw1);
+                                c.rdd, c.w, c, uw0, uw1, cw0, cw1);
             }
             // faces are counted by the cell that holds them: x faces by row i,
-            // y and diagonal faces by row i-1
+            // y and diagonal faces by row i-1; volume caps of the halves the
+            // exact re-evaluation does not redo
             const bool ownA = G.out_lane && i >= G.r0 && i < G.r1;
             const bool ownB = G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1;
+            if (ownA)
+                ss.capn += (unsigned)(cx0 && !ux0) + (unsigned)(cx1 && !ux1);
+            if (ownB) {
+                ss.capn += (unsigned)(cy0 && !uy0) + (unsigned)(cy1 && !uy1);
+                if constexpr (K == 8)
+                    ss.capn += (unsigned)(ce0 && !ue0) + (unsigned)(ce1 && !ue1) +
+                               (unsigned)(cw0 && !uw0) + (unsigned)(cw1 && !uw1);
+            }
             if constexpr (MATH == MATH_EXACT) {
                 bool any = ux0 || ux1 || uy0 || uy1;
                 if constexpr (K == 8)
@@ -461,14 +535,6 @@ struct PairSweep {
                                 ss.capn += o.cap;
                         }
                     }
-                }
-            } else {
-                if (ownA)
-                    ss.capn += (unsigned)ux0 + (unsigned)ux1;
-                if (ownB) {
-                    ss.capn += (unsigned)uy0 + (unsigned)uy1;
-                    if constexpr (K == 8)
-                        ss.capn += (unsigned)ue0 + (unsigned)ue1 + (unsigned)uw0 + (unsigned)uw1;
                 }
             }
             R.X[S0] = X;
@@ -769,10 +835,8 @@ struct PairSweep {
         c.half = bc2(0.5f);
         c.nmin = bc2(1e-12f);
         c.vcrK = bc2(0.99999905f);
-        // exact mode: below A/(2K dt) by more than the roundings of the
-        // estimate, so a face whose |dL| * capK exceeds Qm is surely not
-        // capped; fast mode: RN(1/(2K dt)), the cap being (|dL| A) capK
-        c.capK = MATH == MATH_EXACT ? bc2(k.A * k.rden * 0.99999809f) : bc2(k.rden);
+        c.den = bc2(k.den);
+        c.rden = bc2(k.rden);
         c.tau_l = k.tau_l;
         c.tau_h = k.tau_h;
 
@@ -828,6 +892,12 @@ struct PairSweep {
             for (int i = i0; i < i0 + n_it; i++) {
                 iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
                 rotate_ring<K>(R);
+            }
+        } else if constexpr (FCAB_PAIR_UNROLL == 2) {
+            for (int i = i0; i < i0 + n_it; i += 2) {
+                iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);
+                iter<1, TMA>(R, G, c, sv, rk, kp, ss, i + 1, lane);
+                rotate_ring2<K>(R);
             }
         } else {
             for (int i = i0; i < i0 + n_it; i += 4) {

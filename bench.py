@@ -374,6 +374,7 @@ def main() -> int:
     if world > 1:
         dist.barrier()
     l0 = sess.launches()
+    fp0 = sess.stats()["dt_full_passes"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
@@ -384,6 +385,7 @@ def main() -> int:
     launches = sess.launches() - l0
     ms = e0.elapsed_time(e1)
     st = sess.stats()
+    full_passes = st["dt_full_passes"] - fp0
     active = st["step"] == args.warmup + args.steps
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -403,7 +405,12 @@ def main() -> int:
             "frac": achieved / (peak or 6650.0), "traffic": profile_traffic(),
             "peak_source": "measured" if peak else "fallback",
             "bytes_per_cell": bytes_per_cell, "kernel": "k_step",
-            "time": "CUDA events around the timed steps on the session stream"}
+            "time": "CUDA events around the timed steps on the session stream: one k_step "
+                    "launch per step; the only other kernel in the region is the full velocity "
+                    "pass that k_step tail-launches on a step whose dt seed missed "
+                    "(full_velocity_passes of them, about 0.2 ms each), so achieved "
+                    "understates k_step's own rate by that share",
+            "full_velocity_passes": int(full_passes)}
 
     out = {"metric": METRIC, "value": value, "unit": "Gcell/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,

@@ -91,6 +91,13 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
     b->key.math = m0->cfg.math;
     b->key.rainf = m0->rain_field ? 1 : 0;
     b->key.landonly = m0->landonly ? 1 : 0;
+    // the pair sweep addresses the fields with 32-bit element offsets
+    if (b->key.landonly && b->key.cpl == 2)
+        for (int i = 0; i < n; i++) {
+            const FcabSim *s = members[i];
+            if ((long long)(s->cfg.nrows + s->hn + s->hs + 2 * PADR) * s->pitch >= (1ll << 31))
+                b->key.cpl = 1;
+        }
     if (!lookup_batch_f32(b->key, &b->L)) {
         delete b;
         return bfail(FCAB_ERR_ARG, "fcab_batch_create: no compiled batch variant");

@@ -86,10 +86,12 @@ __device__ __forceinline__ f2 min2(f2 a, f2 b)
 {
     return mk2(fminf(lo2(a), lo2(b)), fminf(hi2(a), hi2(b)));
 }
+// -a per half, as (-0) - a: exact for every number and both zeros (one
+// packed add instead of two integer operations)
 __device__ __forceinline__ f2 neg2(f2 a)
 {
     f2 r;
-    r.u = a.u ^ 0x8000000080000000ull;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.u) : "l"(0x8000000080000000ull), "l"(a.u));
     return r;
 }
 __device__ __forceinline__ f2 abs2(f2 a)

@@ -1150,11 +1150,15 @@ __device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVa
 namespace fcab {
 
 // The pair sweep runs the FP32 all-LAND grids at two columns per lane;
-// every other variant runs sweep_segment.
+// every other variant runs sweep_segment (all of them with
+// FCAB_PAIR_SWEEP=0, a build option for comparing the two).
+#ifndef FCAB_PAIR_SWEEP
+#define FCAB_PAIR_SWEEP 1
+#endif
 template <typename T, int CPL, bool LANDONLY>
 __host__ __device__ constexpr bool use_pair_sweep()
 {
-    return sizeof(T) == 4 && CPL == 2 && LANDONLY;
+    return FCAB_PAIR_SWEEP && sizeof(T) == 4 && CPL == 2 && LANDONLY;
 }
 
 // Launch shape of the step kernel: threads per CTA and the resident warps

@@ -121,66 +121,89 @@ __device__ __forceinline__ f2 vcrit2(f2 g, f2 hf, bool &unsure0, bool &unsure1)
 // Discharge a -> b of two faces (one per half) between all-LAND cells with
 // old levels La, Lb, elevations za, zb and Manning n na, nb, centre distance
 // d (rd = RN(1/d)) and width w (FloodCA src/kernels/physics.h:51-125), with
-// the critical-velocity and volume caps. `cap0`/`cap1`: live halves whose
-// volume cap binds. MATH_EXACT: every operation rounded as the reference's;
-// `un0`/`un1` flag live halves whose value the exact scalar formula must
-// settle (a cube root or critical velocity near a rounding midpoint, or out
-// of range). MATH_FAST: hardware approximations throughout; no flags.
+// the critical-velocity and volume caps, in three parts so that the faces of
+// a row run as one block of independent work: face2_v (the Manning velocity;
+// `cr` flags live halves whose v may reach the critical velocity), then, in
+// one branch for all faces of the row when any lane has such a half,
+// face2_crit (v = min(v, RN(sqrt(g hf)))), then face2_q (discharge, volume
+// cap). MATH_EXACT: every operation rounded as the reference's; `un` flags
+// live halves whose value the exact scalar formula must settle (a cube root
+// or critical velocity near a rounding midpoint, or out of range).
+// MATH_FAST: hardware approximations throughout, no flags.
+struct Face2 {
+    f2 dL, adL, hf, v;
+    bool live0, live1, cr0, cr1, un0, un1;
+};
+
 template <int MATH>
-__device__ __forceinline__ f2 face2(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2 d, f2 rd, f2 w,
-                                    const PairK &c, bool &un0, bool &un1, bool &cap0, bool &cap1)
+__device__ __forceinline__ Face2 face2_v(f2 La, f2 Lb, f2 za, f2 zb, f2 na, f2 nb, f2 d, f2 rd,
+                                         const PairK &c)
 {
-    const f2 dL = sub2(La, Lb);
+    Face2 f;
+    f.dL = sub2(La, Lb);
     const f2 Lmx = max2(La, Lb);
-    const f2 adL = sub2(Lmx, min2(La, Lb));        // |dL|, the same rounding
-    const f2 hf = sub2(Lmx, max2(za, zb));
+    f.adL = sub2(Lmx, min2(La, Lb));        // |dL|, the same rounding
+    f.hf = sub2(Lmx, max2(za, zb));
     float a0, a1, h0, h1;
-    sp2(adL, a0, a1);
-    sp2(hf, h0, h1);
-    const bool live0 = a0 >= c.tau_l && h0 >= c.tau_h;
-    const bool live1 = a1 >= c.tau_l && h1 >= c.tau_h;
+    sp2(f.adL, a0, a1);
+    sp2(f.hf, h0, h1);
+    f.live0 = a0 >= c.tau_l && h0 >= c.tau_h;
+    f.live1 = a1 >= c.tau_l && h1 >= c.tau_h;
     const f2 nf = max2(mul2(c.half, add2(na, nb)), c.nmin);
-    f2 Qm, Qc;
     if constexpr (MATH == MATH_EXACT) {
         const f2 rnf = rcp2_nr(nf);
-        const f2 sq = sqrt2_nr(div2_mk(adL, d, rd));
+        const f2 sq = sqrt2_nr(div2_mk(f.adL, d, rd));
         bool s0, s1;
-        const f2 cb = cbrt_sq2(hf, s0, s1);
-        f2 v = mul2(mul2(rnf, cb), sq);
+        const f2 cb = cbrt_sq2(f.hf, s0, s1);
+        f.v = mul2(mul2(rnf, cb), sq);
         // v^2 < g hf (1 - 1e-6) leaves v surely below the critical velocity
-        const f2 v2 = mul2(v, v);
-        const f2 pm = mul2(mul2(c.g, hf), c.vcrK);
-        const bool cr0 = live0 && !(lo2(v2) < lo2(pm));
-        const bool cr1 = live1 && !(hi2(v2) < hi2(pm));
-        bool vu0 = false, vu1 = false;
-        if (__any_sync(0xffffffffu, cr0 || cr1)) {
-            const f2 vcr = vcrit2(c.g, hf, vu0, vu1);
-            v = sel2(cr0, cr1, min2(v, vcr), v);
-            vu0 = cr0 && vu0;
-            vu1 = cr1 && vu1;
-        }
-        Qm = mul2(mul2(v, hf), w);
-        Qc = div2_mk(mul2(adL, c.A), c.den, c.rden);    // RN(RN(|dL| A) / (2K dt))
-        un0 = live0 && (s0 || vu0);
-        un1 = live1 && (s1 || vu1);
+        const f2 v2 = mul2(f.v, f.v);
+        const f2 pm = mul2(mul2(c.g, f.hf), c.vcrK);
+        f.cr0 = f.live0 && !(lo2(v2) < lo2(pm));
+        f.cr1 = f.live1 && !(hi2(v2) < hi2(pm));
+        f.un0 = f.live0 && s0;
+        f.un1 = f.live1 && s1;
     } else {
         const f2 rnf = rcp_2(nf);
-        const f2 S = mul2(adL, rd);
+        const f2 S = mul2(f.adL, rd);
         const f2 sq = mul2(S, rsqrt_2(S));
-        const f2 cb = ex2_2(mul2(lg2_2(hf), bc2(0.666666687f)));
+        const f2 cb = ex2_2(mul2(lg2_2(f.hf), bc2(0.666666687f)));
         f2 v = mul2(mul2(rnf, cb), sq);
-        const f2 p = mul2(c.g, hf);
+        const f2 p = mul2(c.g, f.hf);
         const f2 vcr = mul2(p, rsqrt_2(p));
         const f2 v2 = mul2(v, v);
-        v = sel2(lo2(v2) > lo2(p), hi2(v2) > hi2(p), vcr, v);
-        Qm = mul2(mul2(v, hf), w);
-        Qc = mul2(mul2(adL, c.A), c.rden);
-        un0 = un1 = false;
+        f.v = sel2(lo2(v2) > lo2(p), hi2(v2) > hi2(p), vcr, v);
+        f.cr0 = f.cr1 = f.un0 = f.un1 = false;
     }
-    cap0 = live0 && lo2(Qc) < lo2(Qm);
-    cap1 = live1 && hi2(Qc) < hi2(Qm);
-    const f2 Q = copysign2(min2(Qm, Qc), dL);
-    return sel2(live0, live1, Q, bc2(0.0f));
+    return f;
+}
+
+// v = min(v, RN(sqrt(g hf))) on the flagged halves (exact mode)
+__device__ __forceinline__ void face2_crit(Face2 &f, const PairK &c)
+{
+    bool vu0, vu1;
+    const f2 vcr = vcrit2(c.g, f.hf, vu0, vu1);
+    f.v = sel2(f.cr0, f.cr1, min2(f.v, vcr), f.v);
+    f.un0 = f.un0 || (f.cr0 && vu0);
+    f.un1 = f.un1 || (f.cr1 && vu1);
+}
+
+// Q = sign(dL) min(v hf w, RN(RN(|dL| A) / (2K dt))); cap: live halves
+// whose volume cap binds
+template <int MATH>
+__device__ __forceinline__ f2 face2_q(const Face2 &f, f2 w, const PairK &c, bool &cap0,
+                                      bool &cap1)
+{
+    const f2 Qm = mul2(mul2(f.v, f.hf), w);
+    f2 Qc;
+    if constexpr (MATH == MATH_EXACT)
+        Qc = div2_mk(mul2(f.adL, c.A), c.den, c.rden);
+    else
+        Qc = mul2(mul2(f.adL, c.A), c.rden);
+    cap0 = f.live0 && lo2(Qc) < lo2(Qm);
+    cap1 = f.live1 && hi2(Qc) < hi2(Qm);
+    const f2 Q = copysign2(min2(Qm, Qc), f.dL);
+    return sel2(f.live0, f.live1, Q, bc2(0.0f));
 }
 
 // Exact re-evaluation of the flagged halves of a face pair with the scalar
@@ -299,7 +322,7 @@ struct PairRing {
 struct PairSeg {
     const float *gz, *gn, *hin, *gcr;
     float *hout, *ghmax, *gtmax;
-    long long pitch, colo;
+    int pitch, colo;                    // 32-bit element offsets (grids checked on the host)
     int nr, nc, r0, r1, r_lo, r_hi;
     int cbase, edges;                   // open edges: bit 0 N, 1 S, 2 W, 3 E (0: closed)
     bool out_lane, edge_strip, col0ok, col1ok;
@@ -310,7 +333,7 @@ struct PairSeg {
     uint32_t *phase;                    // barrier phase bits of the warp (persist over segments)
     int i0, blk, tx;                    // first row, current block, x of the strip
     bool tma_err;
-    long long o1;                       // element offset of row i+1 in the current iteration
+    int o1;                             // element offset of row i+1 in the current iteration
 };
 
 // The ring viewed one row further: slot q takes slot q+1's registers.
@@ -422,12 +445,12 @@ struct PairSweep {
         constexpr int Sm2 = (J + 2) & 3;  // row i-2
         constexpr int Sm3 = (J + 1) & 3;  // row i-3
         constexpr int Sm4 = J & 3;        // row i-4
-        const long long pitch = G.pitch;
+        const int pitch = G.pitch;
         const f2 z0 = bc2(0.0f);
 
         // ---- loads: row i+1, and hmax / rain field of row i-1
         {
-            const long long off = G.o1;
+            const int off = G.o1;
             G.o1 += pitch;
             if constexpr (TMA) {
                 // row i+1 is row i+1-i0 of the stream: a new block every 8
@@ -444,17 +467,17 @@ struct PairSweep {
                 R.z[S1] = ld2(G.gz + off);
                 R.h[S1] = ld2(G.hin + off);
                 R.n[S1] = ld2(G.gn + off);
-                const long long offa =
-                    i + 1 + PF_ROWS <= G.nr + PADR - 1
-                        ? off + PF_ROWS * pitch
-                        : (long long)(G.nr + 2 * PADR - 1) * pitch + G.colo;
+                const int offa = i + 1 + PF_ROWS <= G.nr + PADR - 1
+                                     ? off + PF_ROWS * pitch
+                                     : (G.nr + 2 * PADR - 1) * pitch + G.colo;
                 prefetch_l2(G.gz + offa);
                 prefetch_l2(G.hin + offa);
                 prefetch_l2(G.gn + offa);
             }
-            const long long off1 = off - 2 * pitch;
-            if (G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1)
-                R.hm[Sm1] = ld2_rw(G.ghmax + off1);
+            const int off1 = off - 2 * pitch;
+            // every ring slot is written on every row, so no register of an
+            // older row stays live through the rotation
+            R.hm[Sm1] = G.out_lane && i - 1 >= G.r0 && i - 1 < G.r1 ? ld2_rw(G.ghmax + off1) : z0;
             if constexpr (RAINF)
                 R.cr[Sm1] = ld2(G.gcr + off1);
         }
@@ -463,22 +486,45 @@ struct PairSweep {
         {
             R.L[S0] = add2(R.z[S0], R.h[S0]);
             const f2 zr = right2(R.z[S0]), Lr = right2(R.L[S0]), nrr = right2(R.n[S0]);
-            bool ux0, ux1, uy0, uy1, cx0, cx1, cy0, cy1;
-            f2 X = face2<MATH>(R.L[S0], Lr, R.z[S0], zr, R.n[S0], nrr, c.dx, c.rdx, c.w, c,
-                               ux0, ux1, cx0, cx1);
-            f2 Y = face2<MATH>(R.L[Sm1], R.L[S0], R.z[Sm1], R.z[S0], R.n[Sm1], R.n[S0], c.dx, c.rdx,
-                               c.w, c, uy0, uy1, cy0, cy1);
-            f2 E = z0, W = z0;
-            bool ue0 = false, ue1 = false, uw0 = false, uw1 = false;
-            bool ce0 = false, ce1 = false, cw0 = false, cw1 = false;
+            Face2 fx = face2_v<MATH>(R.L[S0], Lr, R.z[S0], zr, R.n[S0], nrr, c.dx, c.rdx, c);
+            Face2 fy = face2_v<MATH>(R.L[Sm1], R.L[S0], R.z[Sm1], R.z[S0], R.n[Sm1], R.n[S0], c.dx,
+                                     c.rdx, c);
+            Face2 fe, fw;
             if constexpr (K == 8) {
                 R.zr[S0] = zr;
                 R.Lr[S0] = Lr;
                 R.nr[S0] = nrr;
-                E = face2<MATH>(R.L[Sm1], Lr, R.z[Sm1], zr, R.n[Sm1], nrr, c.dd, c.rdd, c.w, c, ue0,
-                                ue1, ce0, ce1);
-                W = face2<MATH>(R.Lr[Sm1], R.L[S0], R.zr[Sm1], R.z[S0], R.nr[Sm1], R.n[S0], c.dd,
-                                c.rdd, c.w, c, uw0, uw1, cw0, cw1);
+                fe = face2_v<MATH>(R.L[Sm1], Lr, R.z[Sm1], zr, R.n[Sm1], nrr, c.dd, c.rdd, c);
+                fw = face2_v<MATH>(R.Lr[Sm1], R.L[S0], R.zr[Sm1], R.z[S0], R.nr[Sm1], R.n[S0], c.dd,
+                                   c.rdd, c);
+            }
+            if constexpr (MATH == MATH_EXACT) {
+                bool crit = fx.cr0 || fx.cr1 || fy.cr0 || fy.cr1;
+                if constexpr (K == 8)
+                    crit = crit || fe.cr0 || fe.cr1 || fw.cr0 || fw.cr1;
+                if (__any_sync(0xffffffffu, crit)) {
+                    face2_crit(fx, c);
+                    face2_crit(fy, c);
+                    if constexpr (K == 8) {
+                        face2_crit(fe, c);
+                        face2_crit(fw, c);
+                    }
+                }
+            }
+            bool cx0, cx1, cy0, cy1;
+            f2 X = face2_q<MATH>(fx, c.w, c, cx0, cx1);
+            f2 Y = face2_q<MATH>(fy, c.w, c, cy0, cy1);
+            const bool ux0 = fx.un0, ux1 = fx.un1, uy0 = fy.un0, uy1 = fy.un1;
+            f2 E = z0, W = z0;
+            bool ue0 = false, ue1 = false, uw0 = false, uw1 = false;
+            bool ce0 = false, ce1 = false, cw0 = false, cw1 = false;
+            if constexpr (K == 8) {
+                E = face2_q<MATH>(fe, c.w, c, ce0, ce1);
+                W = face2_q<MATH>(fw, c.w, c, cw0, cw1);
+                ue0 = fe.un0;
+                ue1 = fe.un1;
+                uw0 = fw.un0;
+                uw1 = fw.un1;
             }
             // faces are counted by the cell that holds them: x faces by row i,
             // y and diagonal faces by row i-1; volume caps of the halves the
@@ -561,6 +607,7 @@ struct PairSweep {
                 out = sub2(out, min2(R.W[Sm2], z0));
             }
             R.ko[Sm1] = 0u;
+            R.qo[Sm1] = z0;
             if (G.edges) {
                 const bool erow = (r == 0 && (G.edges & 1)) || (r == G.nr - 1 && (G.edges & 2));
                 if (erow || G.edge_strip) {
@@ -696,6 +743,8 @@ struct PairSweep {
                     ef |= 1u;
                 if (cell1 && hi2(hu) >= c.tau_h && !(t && hi2(gh) <= G.thr2c))
                     ef |= 2u;
+            }
+            {
                 const f2 n2 = mul2(R.n[Sm2], R.n[Sm2]);
                 R.n6[Sm2] = mul2(mul2(n2, n2), n2);
             }
@@ -705,7 +754,7 @@ struct PairSweep {
             const bool rise0 = cell0 && lo2(hu) > lo2(hmo);
             const bool rise1 = cell1 && hi2(hu) > hi2(hmo);
             if (row_out && G.out_lane) {
-                const long long off2 = G.o1 - 4 * pitch;        // row i-2
+                const int off2 = G.o1 - 4 * pitch;              // row i-2
                 st2(G.hout + off2, hkeep);
                 if (rise0 || rise1) {
                     st2(G.ghmax + off2, sel2(rise0, rise1, hu, hmo));
@@ -736,7 +785,7 @@ struct PairSweep {
                 const bool erow = (r == 0 && (G.edges & 1)) || (r == G.nr - 1 && (G.edges & 2));
                 if (erow || G.edge_strip) {
                     // the open virtual neighbour z - S_bnd*dx, h = 0 (physics.h:183-189)
-                    const long long off3 = G.o1 - 5 * pitch;    // row i-3
+                    const int off3 = G.o1 - 5 * pitch;          // row i-3
                     const f2 z3 = ld2(G.gz + off3);
                     const f2 dv = abs2(sub2(la, sub2(z3, bc2(sv.k.S_bnd * sv.k.dx))));
 #pragma unroll
@@ -759,7 +808,7 @@ struct PairSweep {
             const bool x0 = (ef & 1u) && (lo2(lhs) >= lo2(rhs) || lo2(lhs) < 1e-30f);
             const bool x1 = (ef & 2u) && (hi2(lhs) >= hi2(rhs) || hi2(lhs) < 1e-30f);
             if (__any_sync(0xffffffffu, x0 || x1)) {
-                const long long off3 = G.o1 - 5 * pitch;        // row i-3
+                const int off3 = G.o1 - 5 * pitch;              // row i-3
                 const f2 n3 = ld2(G.gn + off3);
                 float vm = ss.vmax;
                 if (x0 || x1)
@@ -800,7 +849,7 @@ struct PairSweep {
         G.hout = sv.hout;
         G.ghmax = g.hmax;
         G.gtmax = g.tmax;
-        G.pitch = g.pitch;
+        G.pitch = (int)g.pitch;
         G.nr = g.nr;
         G.nc = g.nc;
         G.r0 = r0;
@@ -808,7 +857,7 @@ struct PairSweep {
         G.r_lo = g.r_lo;
         G.r_hi = g.r_hi;
         G.cbase = strip * Gm::OW - Gm::HL + lane * 2;
-        G.colo = (long long)(G.cbase + PADC);
+        G.colo = G.cbase + PADC;
         G.out_lane = lane * 2 >= Gm::HL && lane * 2 < Gm::HL + Gm::OW;
         G.col0ok = G.cbase >= 0 && G.cbase < g.nc;
         G.col1ok = G.cbase + 1 >= 0 && G.cbase + 1 < g.nc;
@@ -882,12 +931,12 @@ struct PairSweep {
             R.n[0] = lds2(G.srow + 2 * TMA_FIELD_B);
             G.srow += 256;
         } else {
-            const long long off = (long long)(i0 + PADR) * G.pitch + G.colo;
+            const int off = (i0 + PADR) * G.pitch + G.colo;
             R.z[0] = ld2(G.gz + off);
             R.h[0] = ld2(G.hin + off);
             R.n[0] = ld2(G.gn + off);
         }
-        G.o1 = (long long)(i0 + 1 + PADR) * G.pitch + G.colo;
+        G.o1 = (i0 + 1 + PADR) * G.pitch + G.colo;
         if constexpr (FCAB_PAIR_UNROLL == 1) {
             for (int i = i0; i < i0 + n_it; i++) {
                 iter<0, TMA>(R, G, c, sv, rk, kp, ss, i, lane);

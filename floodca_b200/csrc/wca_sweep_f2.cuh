@@ -754,15 +754,15 @@ struct PairSweep {
             const bool rise0 = cell0 && lo2(hu) > lo2(hmo);
             const bool rise1 = cell1 && hi2(hu) > hi2(hmo);
             if (row_out && G.out_lane) {
+                // hmax is written back whether or not it rose (no divergent
+                // branch; the loaded value where it did not), tmax where it rose
                 const int off2 = G.o1 - 4 * pitch;              // row i-2
                 st2(G.hout + off2, hkeep);
-                if (rise0 || rise1) {
-                    st2(G.ghmax + off2, sel2(rise0, rise1, hu, hmo));
-                    if (rise0)
-                        G.gtmax[off2] = sv.tmax_val;
-                    if (rise1)
-                        G.gtmax[off2 + 1] = sv.tmax_val;
-                }
+                st2(G.ghmax + off2, sel2(rise0, rise1, hu, hmo));
+                if (rise0)
+                    G.gtmax[off2] = sv.tmax_val;
+                if (rise1)
+                    G.gtmax[off2 + 1] = sv.tmax_val;
             }
         }
 

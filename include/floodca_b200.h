@@ -127,9 +127,13 @@ extern "C" {
  * flag g->edge_{n,s,w,e} is honoured (the reference CUDA path treats all four
  * edges as open); a CUDA failure returns -2 instead of exit(1); a fixed-step
  * run (cfg->steps > 0) whose step would have dt <= 0 stops instead of
- * looping forever. Returns 0, -1 on a bad block shape (same check as the
- * reference), -2 on a device error. The run's device buffers stay cached
- * for later runs (fcab_release_cached_memory frees them). */
+ * looping forever; run parameters the step cannot use (see fcab_sim_create)
+ * and a non-finite z, h, n, C or Rday on a LAND cell are refused with -2.
+ * A forcing-day file that is missing or short ends the run there with
+ * acc->t = T_sim and returns 0, as the reference does. Returns 0, -1 on a
+ * bad block shape (same check as the reference), -2 on a refused input or a
+ * device error. The run's device buffers stay cached for later runs
+ * (fcab_release_cached_memory frees them). */
 FCAB_API int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *tm);
 
 /* Replaces fca_cuda_device_name (src/cuda/kernels.cu:606-615). */
@@ -221,7 +225,15 @@ typedef struct FcabSim FcabSim;
 FCAB_API void fcab_config_defaults(FcabConfig *cfg, int nrows, int ncols);
 
 /* Creates a session on the current device. stream is a cudaStream_t (NULL:
- * the session creates its own). Returns 0 or a negative code. */
+ * the session creates its own). Returns 0 or a negative code. Before any
+ * CUDA call it refuses (FCAB_ERR_ARG, message in fcab_last_error) an empty
+ * or too large grid, K other than 4 or 8, U < 1, unknown precision, math,
+ * boundary or hyetograph, non-positive or non-finite dx, g, alpha, dt_max
+ * or dt_min, negative or non-finite tau_h / tau_l, non-finite z_sea, S_bnd,
+ * T_sim, out_every, D_h, phi or rain_end, negative max_steps or seg_rows,
+ * cols_per_lane other than 0, 1, 2 or 4, and a non-finite inflow
+ * hydrograph. fcab_sim_upload refuses a non-finite z, h, n, C or Rday on a
+ * LAND cell. */
 FCAB_API int fcab_sim_create(FcabSim **out, const FcabConfig *cfg, void *stream);
 
 /* Uploads row-major host fields of nrows*ncols values (float, or double for

@@ -1146,6 +1146,7 @@ __device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVa
 }  // namespace fcab
 
 #include "wca_sweep_f2.cuh"
+#include "wca_sweep_f4.cuh"
 
 namespace fcab {
 
@@ -1159,6 +1160,13 @@ template <typename T, int CPL, bool LANDONLY>
 __host__ __device__ constexpr bool use_pair_sweep()
 {
     return FCAB_PAIR_SWEEP && sizeof(T) == 4 && CPL == 2 && LANDONLY;
+}
+// The four-column sweep (two pairs per lane) runs the FP32 all-LAND K = 4
+// grids at four columns per lane.
+template <typename T, int K, int CPL, bool LANDONLY>
+__host__ __device__ constexpr bool use_quad_sweep()
+{
+    return FCAB_PAIR_SWEEP && sizeof(T) == 4 && CPL == 4 && K == 4 && LANDONLY;
 }
 
 // Launch shape of the step kernel: threads per CTA and the resident warps
@@ -1202,11 +1210,19 @@ __host__ __device__ constexpr int pair_warps()
 {
     return K == 8 ? FCAB_PAIR_WARPS_K8 : FCAB_PAIR_WARPS;
 }
+// Resident warps per SM of the four-column sweep (twice the pair sweep's
+// state per lane: up to 255 registers at 8 warps)
+#ifndef FCAB_QUAD_WARPS
+#define FCAB_QUAD_WARPS 8
+#endif
 template <typename T, int K, int CPL, int MATH, bool LANDONLY>
 __host__ __device__ constexpr int step_blocks_per_sm()
 {
-    return use_pair_sweep<T, CPL, LANDONLY>() ? pair_warps<K>() / (step_threads<CPL, MATH>() / 32)
-                                              : step_min_blocks<K, CPL, MATH>();
+    return use_pair_sweep<T, CPL, LANDONLY>()
+               ? pair_warps<K>() / (step_threads<CPL, MATH>() / 32)
+               : use_quad_sweep<T, K, CPL, LANDONLY>()
+                     ? FCAB_QUAD_WARPS / (step_threads<CPL, MATH>() / 32)
+                     : step_min_blocks<K, CPL, MATH>();
 }
 
 template <typename T, int K, int MATH>
@@ -1243,6 +1259,11 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
     extern __shared__ __align__(1024) unsigned char fcab_dsm[];
     uint32_t ring = 0u, bars = 0u;
     const int wib = threadIdx.x >> 5;
+    if constexpr (use_quad_sweep<T, K, CPL, LANDONLY>()) {
+        if (threadIdx.x == 0)
+            sk = sv.k;
+        __syncthreads();
+    }
     if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
         if (threadIdx.x == 0) {
             sk = sv.k;
@@ -1276,6 +1297,8 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
                                                  bars, &tphase[wib], &bad);
             if (bad && lane == 0)
                 tma_bad = 1;
+        } else if constexpr (use_quad_sweep<T, K, CPL, LANDONLY>()) {
+            QuadSweep<AccT, MATH, RAINF>::run(g, rk, sv, &sk, strip, r0, r1, lane, ss);
         } else {
             sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane,
                                                                   ss);

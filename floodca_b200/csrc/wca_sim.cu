@@ -672,9 +672,10 @@ static int resolve_variant(FcabSim *s)
     key.math = s->cfg.precision == FCAB_PREC_F32 ? s->cfg.math : FCAB_MATH_EXACT;
     key.rainf = s->rain_field ? 1 : 0;
     key.landonly = s->landonly ? 1 : 0;
-    // the pair sweep (FP32, all-LAND, two columns per lane) addresses the
-    // fields with 32-bit element offsets: larger grids take one column per lane
-    if (s->esize == 4 && key.landonly && key.cpl == 2 &&
+    // the pair and four-column sweeps (FP32, all-LAND, two or four columns
+    // per lane) address the fields with 32-bit element offsets: larger grids
+    // take one column per lane
+    if (s->esize == 4 && key.landonly && (key.cpl == 2 || key.cpl == 4) &&
         (long long)(s->cfg.nrows + s->hn + s->hs + 2 * PADR) * s->pitch >= (1ll << 31))
         key.cpl = s->cpl = 1;
     bool ok = key.prec == FCAB_PREC_F32 ? lookup_f32(key, &s->L)

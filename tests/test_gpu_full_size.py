@@ -7,9 +7,10 @@ parity flags), FP32 bit for bit.
   warm start (20 mm on every cell, the state bench.py times);
 * config 3, 2048 x 2048 with 100 mm/h rain: the first 300 steps.
 
-Each runs with one column per lane and with two (the packed pair sweep the
-benchmark uses on these all-LAND grids). The reference core runs on every
-host core (OpenMP); 200 warm 4096^2 steps take it about 20 s."""
+Each runs with one, two and four columns per lane (the packed sweeps on
+pairs of columns, one or two pairs per lane, on these all-LAND grids). The
+reference core runs on every host core (OpenMP); 200 warm 4096^2 steps take
+it about 20 s."""
 import os
 
 import numpy as np
@@ -45,7 +46,7 @@ def test_config2_full_size_equals_reference(start):
     p = p.with_(steps=200)
     ref = refcore.run(d, p, kind="f32", threads=_threads())
     assert ref["V_in"] > 0.0
-    for cpl in (1, 2):
+    for cpl in (1, 2, 4):
         _check(run_session(d, p, precision="f32", cols_per_lane=cpl), ref)
 
 
@@ -54,5 +55,5 @@ def test_config3_full_size_equals_reference():
     assert d.shape == (2048, 2048)
     p = p.with_(steps=300)
     ref = refcore.run(d, p, kind="f32", threads=_threads())
-    for cpl in (1, 2):
+    for cpl in (1, 2, 4):
         _check(run_session(d, p, precision="f32", cols_per_lane=cpl), ref)

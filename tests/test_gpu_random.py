@@ -6,8 +6,9 @@ uniform hyetographs, fixed step counts or a simulated time.
 
 Each grid also runs as an all-LAND grid (SEA and WALL cells turned to LAND),
 which takes the all-LAND kernels, with the random C*Rday field as a per-cell
-rain field. Both lane widths run: one column per lane and two (the packed
-pair sweep on all-LAND grids). FP32 must equal the reference bit for bit;
+rain field. Every lane width runs: one column per lane, two (the packed
+pair sweep on all-LAND grids) and four (two pairs per lane on all-LAND K = 4
+grids). FP32 must equal the reference bit for bit;
 FP64 depths within 1e-12 m and times within 1e-9 s (the device's and glibc's
 double cube roots may differ in the last bit)."""
 import numpy as np
@@ -46,7 +47,7 @@ def _check(r, ref, kind):
 def test_session_equals_reference_random(seed, kind):
     dom, p = _case(1000 + seed)
     ref = refcore.run(dom, p, kind=kind)
-    for cpl in (1, 2):
+    for cpl in (1, 2, 4):
         _check(run_session(dom, p, precision=kind, cols_per_lane=cpl), ref, kind)
 
 
@@ -56,5 +57,5 @@ def test_all_land_session_equals_reference_random(seed):
     dom = dom.copy()
     dom.mask[:] = 0
     ref = refcore.run(dom, p, kind="f32")
-    for cpl in (1, 2):
+    for cpl in (1, 2, 4):
         _check(run_session(dom, p, precision="f32", cols_per_lane=cpl), ref, "f32")

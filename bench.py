@@ -373,8 +373,8 @@ def main() -> int:
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    fp0 = sess.stats()["dt_full_passes"]      # (launches k_volume: before the count)
     l0 = sess.launches()
-    fp0 = sess.stats()["dt_full_passes"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)

@@ -262,7 +262,9 @@ extern "C" int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *
     }
     tm->t_d2h = now_s() - ti;
     fcab_sim_destroy(s);
-    return 0;
+    // a forcing day failed to load: the state is where the run stopped (as
+    // the reference leaves it), but the caller is told
+    return rc == 1 ? -3 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -348,7 +350,7 @@ extern "C" int fca_cuda_ens_run(FcaCudaEns *e, FcaGrid *g, const FcaRunCfg *cfg,
     tm->t_d2h += now_s() - ti;
     for (int j = 0; j < e->nthr; j++)
         flooded[j] = (long)fl[j];
-    return 0;
+    return rc == 1 ? -3 : 0;
 }
 
 extern "C" int fca_cuda_ens_counts(FcaCudaEns *e, uint16_t *host)

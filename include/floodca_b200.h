@@ -129,11 +129,13 @@ extern "C" {
  * run (cfg->steps > 0) whose step would have dt <= 0 stops instead of
  * looping forever; run parameters the step cannot use (see fcab_sim_create)
  * and a non-finite z, h, n, C or Rday on a LAND cell are refused with -2.
- * A forcing-day file that is missing or short ends the run there with
- * acc->t = T_sim and returns 0, as the reference does. Returns 0, -1 on a
- * bad block shape (same check as the reference), -2 on a refused input or a
- * device error. The run's device buffers stay cached for later runs
- * (fcab_release_cached_memory frees them). */
+ * A forcing-day file that is missing or short ends the run where that day
+ * begins, with acc->t = T_sim and h, hmax, tmax downloaded as the reference
+ * leaves them, but returns -3 (the reference returns 0, and its CLI then
+ * writes a truncated run as if complete). Returns 0, -1 on a bad block shape
+ * (same check as the reference), -2 on a refused input or a device error,
+ * -3 on a forcing file that failed to load. The run's device buffers stay
+ * cached for later runs (fcab_release_cached_memory frees them). */
 FCAB_API int fca_cuda_run(FcaGrid *g, FcaRunCfg *cfg, FcaAcc *acc, FcaTimers *tm);
 
 /* Replaces fca_cuda_device_name (src/cuda/kernels.cu:606-615). */

@@ -1,10 +1,12 @@
 """Failure paths through the reference-facing fca_cuda_run on the device.
 
-* A forcing day whose file is missing or short ends the run where that day
-  begins, as the reference does (src/cuda/kernels.cu:497-507 and 712-732):
-  fca_cuda_run returns 0, acc.t is set to T_sim, and the state is the state
-  of the steps taken before the failed load (checked against a fixed-step
-  run of the same forcing with every file present).
+* A forcing day whose file is missing, short or unnamed ends the run where
+  that day begins, as the reference's loop does (src/cuda/kernels.cu:497-507
+  and 712-732): acc.t is set to T_sim and the state is the state of the
+  steps taken before the failed load (checked against a fixed-step run of
+  the same forcing with every file present). Unlike the reference, which
+  returns 0 there, fca_cuda_run returns -3, so a caller such as the
+  reference's CLI does not take the truncated run for a complete one.
 * A non-finite z, h, n, C or Rday on a LAND cell makes the upload fail:
   fca_cuda_run returns -2 and fcab_last_error names the field and the cell.
   The reference does not check its inputs; non-finite values would spread
@@ -56,7 +58,7 @@ def _golden_run_ok():
 
 
 @pytest.mark.parametrize("how", ["missing", "short", "empty_name"])
-def test_failed_forcing_day_ends_the_run_like_the_reference(how):
+def test_failed_forcing_day_ends_the_run_and_is_reported(how):
     _, p, _, force = load_case(GOLDEN / "forcing.npz")
     assert len(force) == 2 and p.T_sim > 86400.0
     with tempfile.TemporaryDirectory() as tmp:
@@ -65,7 +67,7 @@ def test_failed_forcing_day_ends_the_run_like_the_reference(how):
             np.asarray(force[1], np.float32).ravel()[:-1].tofile(day1)
         files = [str(Path(tmp) / "rday_0.bin"), "" if how == "empty_name" else str(day1)]
         g, _ = _forcing_grid(tmp, force, files=files)
-        assert g.run() == 0
+        assert g.run() == -3
         r = g.result()
         assert r["t"] == p.T_sim                      # the reference's end marker
         n = r["step"]

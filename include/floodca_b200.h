@@ -186,7 +186,9 @@ typedef struct FcabConfig {
     double inflow_peak;       /* triangular hydrograph: 0 at t=0, peak (m^3/s) at */
     double inflow_t_peak;     /*   inflow_t_peak, 0 at inflow_t_end; added after  */
     double inflow_t_end;      /*   the clamp, before hmax                         */
-    int cols_per_lane;        /* 0 = autotuned; else 1, 2 or 4 */
+    int cols_per_lane;        /* 0 = autotuned (1 or 2); else 1, 2 or 4 (FP32 all-LAND
+                                 grids: 2 runs the packed pair sweep, 4 with K = 4 two
+                                 pairs per lane; padded fields beyond 2^31 elements run 1) */
     int seg_rows;             /* 0 = autotuned; rows per warp segment */
 } FcabConfig;
 

@@ -5,7 +5,7 @@ parity flags), FP32 bit for bit.
 * config 2, 4096 x 4096 with the north-edge point inflow and 30 mm/h rain:
   the first 200 steps from the dry start, and 200 steps from the benchmark's
   warm start (20 mm on every cell, the state bench.py times);
-* config 3, 2048 x 2048 with 100 mm/h rain: the first 300 steps.
+* config 3, 2048 x 2048 with 100 mm/h rain for 3 h: the whole 6 h run.
 
 Each runs with one, two and four columns per lane (the packed sweeps on
 pairs of columns, one or two pairs per lane, on these all-LAND grids). The
@@ -52,8 +52,8 @@ def test_config2_full_size_equals_reference(start):
 
 def test_config3_full_size_equals_reference():
     d, p = synth.config3()
-    assert d.shape == (2048, 2048)
-    p = p.with_(steps=300)
-    ref = refcore.run(d, p, kind="f32", threads=_threads())
+    assert d.shape == (2048, 2048) and p.T_sim == 21600.0 and p.steps == 0
+    ref = refcore.run(d, p, kind="f32", threads=_threads())     # the whole 6 h run
+    assert ref["t"] == pytest.approx(p.T_sim) and ref["step"] > 1000
     for cpl in (1, 2, 4):
         _check(run_session(d, p, precision="f32", cols_per_lane=cpl), ref)

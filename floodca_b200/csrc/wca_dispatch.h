@@ -103,7 +103,7 @@ Launchers make_launchers()
     L.init = &launch_init<T, K, MATH>;
     L.step_fn = (const void *)&k_step<T, AccT, K, CPL, MATH, RAINF, LAND>;
     L.threads = step_threads<CPL, MATH>();
-    L.tma_smem = use_pair_sweep<T, CPL, LAND>() ? tma_smem_bytes(L.threads / 32) : 0;
+    L.tma_smem = use_pair_sweep<T, K, CPL, LAND>() ? tma_smem_bytes(L.threads / 32) : 0;
     return L;
 }
 

@@ -1150,16 +1150,23 @@ __device__ __forceinline__ void publish_sums(StepSums<T, AccT> &ss, const StepVa
 
 namespace fcab {
 
-// The pair sweep runs the FP32 all-LAND grids at two columns per lane;
-// every other variant runs sweep_segment (all of them with
+// The pair sweep runs the FP32 all-LAND K = 4 grids at two columns per
+// lane; every other variant runs sweep_segment (all of them with
 // FCAB_PAIR_SWEEP=0, a build option for comparing the two).
 #ifndef FCAB_PAIR_SWEEP
 #define FCAB_PAIR_SWEEP 1
 #endif
-template <typename T, int CPL, bool LANDONLY>
+// For K = 8 the scalar sweep is the faster of the two (measured at 4096^2
+// on a B200: 24.8 against 23.4 Gcell/s exact, 36.4 against 32.5 fast; the
+// pair sweep's K = 8 face state leaves it 8 warps per SM); FCAB_PAIR_K8=1
+// runs K = 8 on the pair sweep too.
+#ifndef FCAB_PAIR_K8
+#define FCAB_PAIR_K8 0
+#endif
+template <typename T, int K, int CPL, bool LANDONLY>
 __host__ __device__ constexpr bool use_pair_sweep()
 {
-    return FCAB_PAIR_SWEEP && sizeof(T) == 4 && CPL == 2 && LANDONLY;
+    return FCAB_PAIR_SWEEP && sizeof(T) == 4 && CPL == 2 && LANDONLY && (K == 4 || FCAB_PAIR_K8);
 }
 // The four-column sweep (two pairs per lane) runs the FP32 all-LAND K = 4
 // grids at four columns per lane.
@@ -1218,7 +1225,7 @@ __host__ __device__ constexpr int pair_warps()
 template <typename T, int K, int CPL, int MATH, bool LANDONLY>
 __host__ __device__ constexpr int step_blocks_per_sm()
 {
-    return use_pair_sweep<T, CPL, LANDONLY>()
+    return use_pair_sweep<T, K, CPL, LANDONLY>()
                ? pair_warps<K>() / (step_threads<CPL, MATH>() / 32)
                : use_quad_sweep<T, K, CPL, LANDONLY>()
                      ? FCAB_QUAD_WARPS / (step_threads<CPL, MATH>() / 32)
@@ -1264,7 +1271,7 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
             sk = sv.k;
         __syncthreads();
     }
-    if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+    if constexpr (use_pair_sweep<T, K, CPL, LANDONLY>()) {
         if (threadIdx.x == 0) {
             sk = sv.k;
             tma_bad = 0;
@@ -1291,7 +1298,7 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
         const int r0 = (int)(w0 % nr);
         const int r1 = (int)min((long long)nr, (long long)r0 + (w1 - w0));
         w0 += r1 - r0;
-        if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+        if constexpr (use_pair_sweep<T, K, CPL, LANDONLY>()) {
             bool bad = false;
             PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &sk, strip, r0, r1, lane, ss, ring,
                                                  bars, &tphase[wib], &bad);
@@ -1304,7 +1311,7 @@ __global__ void __launch_bounds__(step_threads<CPL, MATH>(),
                                                                   ss);
         }
     }
-    if constexpr (use_pair_sweep<T, CPL, LANDONLY>()) {
+    if constexpr (use_pair_sweep<T, K, CPL, LANDONLY>()) {
         __syncthreads();
         if (threadIdx.x == 0 && tma_bad)
             ctl->err = 3;           // a row tile never arrived; the host reports it
@@ -1365,7 +1372,7 @@ struct BatchQ {
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128, use_pair_sweep<T, CPL, LANDONLY>() ? pair_warps<K>() / 4
+__global__ void __launch_bounds__(128, use_pair_sweep<T, K, CPL, LANDONLY>() ? pair_warps<K>() / 4
                                                                       : (CPL == 2 ? 4 : 1))
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,
@@ -1414,7 +1421,7 @@ k_step_batch(const MemberD<T> *members,
         __syncwarp();
         const StepVals<T> &sv = ssv[wib];
         StepSums<T, AccT> ss;
-        if constexpr (use_pair_sweep<T, CPL, LANDONLY>())
+        if constexpr (use_pair_sweep<T, K, CPL, LANDONLY>())
             PairSweep<AccT, K, MATH, RAINF>::run(g, rk, sv, &ssv[wib].k, strip, r0, r1, lane, ss);
         else
             sweep_segment<T, AccT, K, CPL, MATH, RAINF, LANDONLY>(g, rk, sv, strip, r0, r1, lane,

@@ -29,6 +29,24 @@ __global__ void k_gather_active(const MemberD<float> *members, int n, int *flags
     }
 }
 
+// The loop condition of a window graph: keep stepping while any member is
+// active (running in the current window) and the pass count is below `cap`
+// (a bound on one graph launch; the host launches the graph again if members
+// are still running).
+__global__ void k_batch_cond(const MemberD<float> *members, int n, cudaGraphConditionalHandle h,
+                             unsigned long long *passes, unsigned long long cap)
+{
+    int any = 0;
+    for (int m = threadIdx.x; m < n; m += blockDim.x)
+        any |= members[m].ctl->active != 0;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const unsigned long long k = *passes + 1;
+        *passes = k;
+        cudaGraphSetConditional(h, any && k < cap ? 1u : 0u);
+    }
+}
+
 int bfail(int code, const char *msg)
 {
     set_error(msg);
@@ -52,6 +70,13 @@ struct FcabBatch {
     int total_units = 0, grid = 1, seg = 64;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    // one graph per output window: [open the window], then a conditional
+    // while loop of `wsteps` steps per pass until no member is active
+    cudaGraphExec_t wgraph = nullptr;
+    int wsteps = 0;
+    double wwindow = 0.0;
+    bool wgraph_failed = false;     // conditional graphs unavailable: host-polled loop
+    unsigned long long *d_passes = nullptr;
     long long launches = 0, windows = 0, replays = 0;
 };
 
@@ -146,6 +171,8 @@ extern "C" int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n
     if (e == cudaSuccess)
         e = cudaMallocHost(&b->h_flags, sizeof(int) * n);
     if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_passes, sizeof(unsigned long long));
+    if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_members, md.data(), sizeof(MemberD<float>) * n,
                             cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess)
@@ -175,6 +202,9 @@ extern "C" void fcab_batch_destroy(FcabBatch *b)
         return;
     if (b->graph)
         cudaGraphExecDestroy(b->graph);
+    if (b->wgraph)
+        cudaGraphExecDestroy(b->wgraph);
+    cudaFree(b->d_passes);
     cudaFree(b->d_members);
     cudaFree(b->d_unit_member);
     cudaFree(b->d_need);
@@ -215,53 +245,177 @@ static int batch_graph(FcabBatch *b, int steps)
     return 0;
 }
 
+// Passes of the window loop in one graph launch at most (each `wsteps` steps).
+constexpr unsigned long long WINDOW_PASS_CAP = 1ull << 20;
+
+// One graph per output window: the window's opening (paced runs), then a
+// conditional while node whose body is `steps` batch steps and the loop
+// condition (k_batch_cond), so a window is one graph launch with no host
+// round trip inside it. Returns nonzero (and leaves no graph) when the
+// driver cannot build it.
+static int window_graph(FcabBatch *b, int steps, double window_s)
+{
+    if (b->wgraph && b->wsteps == steps && b->wwindow == window_s)
+        return 0;
+    if (b->wgraph) {
+        cudaGraphExecDestroy(b->wgraph);
+        b->wgraph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    cudaGraphConditionalHandle h = 0;
+    if (e == cudaSuccess)
+        e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    // top level: reset the pass count, open the window
+    if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(b->stream, g, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t le = cudaMemsetAsync(b->d_passes, 0, sizeof(unsigned long long), b->stream);
+        if (le == cudaSuccess && window_s > 0.0)
+            le = b->L.window(b->d_members, b->n, window_s, b->stream);
+        cudaGraph_t gc = nullptr;
+        e = cudaStreamEndCapture(b->stream, &gc);
+        if (e == cudaSuccess)
+            e = le;
+    }
+    // the loop hangs off the last node of the top level
+    std::vector<cudaGraphNode_t> leaves;
+    if (e == cudaSuccess) {
+        size_t nn = 0;
+        e = cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (e == cudaSuccess && nn)
+            e = cudaGraphGetNodes(g, nodes.data(), &nn);
+        for (size_t k = 0; k < nn && e == cudaSuccess; k++) {
+            size_t nd = 0;
+            e = cudaGraphNodeGetDependentNodes(nodes[k], nullptr, &nd);
+            if (e == cudaSuccess && nd == 0)
+                leaves.push_back(nodes[k]);
+        }
+    }
+    // (the parameter struct has no default constructor: zeroed storage)
+    alignas(cudaGraphNodeParams) unsigned char cpb[sizeof(cudaGraphNodeParams)];
+    memset(cpb, 0, sizeof(cpb));
+    cudaGraphNodeParams &cp = *reinterpret_cast<cudaGraphNodeParams *>(cpb);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn = nullptr;
+    if (e == cudaSuccess)
+        e = cudaGraphAddNode(&cn, g, leaves.data(), leaves.size(), &cp);
+    if (e == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t le = cudaSuccess;
+            for (int i = 0; i < steps && le == cudaSuccess; i++) {
+                le = b->L.step(b->d_members, b->d_unit_member, b->total_units, b->d_q, b->d_need,
+                               b->grid, b->stream);
+                if (le == cudaSuccess)
+                    le = b->L.vfull(b->d_members, b->d_need, b->d_q, 2 * 148 * 4, b->stream);
+            }
+            if (le == cudaSuccess) {
+                k_batch_cond<<<1, 256, 0, b->stream>>>(b->d_members, b->n, h, b->d_passes,
+                                                        WINDOW_PASS_CAP);
+                le = cudaGetLastError();
+            }
+            cudaGraph_t bc = nullptr;
+            e = cudaStreamEndCapture(b->stream, &bc);
+            if (e == cudaSuccess)
+                e = le;
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&b->wgraph, g, 0);
+    if (g)
+        cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->wgraph = nullptr;
+        cudaGetLastError();     // clear the (non-sticky) error of the failed build
+        return 1;
+    }
+    b->wsteps = steps;
+    b->wwindow = window_s;
+    return 0;
+}
+
+// Members running / paused at a window end, and the window loop's passes.
+static int poll_members(FcabBatch *b, int *running, int *paused, unsigned long long *passes)
+{
+    k_gather_active<<<(b->n + 127) / 128, 128, 0, b->stream>>>(b->d_members, b->n, b->d_flags);
+    b->launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * b->n, cudaMemcpyDeviceToHost,
+                            b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(passes, b->d_passes, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess)
+        return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+    *running = *paused = 0;
+    for (int i = 0; i < b->n; i++) {
+        *running += b->h_flags[i] == 1;
+        *paused += b->h_flags[i] == 2;
+    }
+    return 0;
+}
+
 extern "C" int fcab_batch_run(FcabBatch *b, double window_s, int graph_steps, int max_windows)
 {
     const bool paced = window_s > 0.0;
     const int steps = graph_steps > 0 ? graph_steps : 16;
-    int rc = batch_graph(b, steps);
-    if (rc)
-        return rc;
+    if (!b->wgraph_failed && window_graph(b, steps, paced ? window_s : 0.0) != 0)
+        b->wgraph_failed = true;
+    const bool wg = !b->wgraph_failed;
     cudaError_t e;
     int opened = 0;
-    if (paced) {
-        e = b->L.window(b->d_members, b->n, window_s, b->stream);
-        if (e != cudaSuccess)
-            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
-        b->launches += 1;
-        b->windows += 1;
-        opened = 1;
-    }
     for (;;) {
-        e = cudaGraphLaunch(b->graph, b->stream);
-        if (e != cudaSuccess)
-            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
-        b->launches += 2 * steps;
-        b->replays += 1;
-        k_gather_active<<<(b->n + 127) / 128, 128, 0, b->stream>>>(b->d_members, b->n,
-                                                                   b->d_flags);
-        b->launches += 1;
-        e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * b->n, cudaMemcpyDeviceToHost,
-                            b->stream);
-        if (e == cudaSuccess)
-            e = cudaStreamSynchronize(b->stream);
-        if (e != cudaSuccess)
-            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
-        int running = 0, paused = 0;
-        for (int i = 0; i < b->n; i++) {
-            running += b->h_flags[i] == 1;
-            paused += b->h_flags[i] == 2;
+        // the window: one graph launch, or its opening kernel before the
+        // host-polled replays below
+        if (wg) {
+            e = cudaGraphLaunch(b->wgraph, b->stream);
+            if (e != cudaSuccess)
+                return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+            b->replays += 1;
+        } else if (paced) {
+            e = b->L.window(b->d_members, b->n, window_s, b->stream);
+            if (e != cudaSuccess)
+                return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
         }
-        if (running)
-            continue;
+        if (paced) {
+            b->launches += 1;
+            b->windows += 1;
+            opened += 1;
+        }
+        int running = 0, paused = 0;
+        unsigned long long passes = 0;
+        int rc = poll_members(b, &running, &paused, &passes);
+        if (rc)
+            return rc;
+        if (wg)
+            b->launches += (long long)passes * (2 * steps + 1);
+        // members still running: no window graph, or its pass cap was hit
+        while (running) {
+            rc = batch_graph(b, steps);
+            if (rc)
+                return rc;
+            e = cudaGraphLaunch(b->graph, b->stream);
+            if (e != cudaSuccess)
+                return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
+            b->launches += 2 * steps;
+            b->replays += 1;
+            rc = poll_members(b, &running, &paused, &passes);
+            if (rc)
+                return rc;
+        }
         if (!paused || !paced || (max_windows > 0 && opened >= max_windows))
             break;
-        e = b->L.window(b->d_members, b->n, window_s, b->stream);
-        if (e != cudaSuccess)
-            return bfail(FCAB_ERR_CUDA, cudaGetErrorString(e));
-        b->launches += 1;
-        b->windows += 1;
-        opened += 1;
     }
     return 0;
 }

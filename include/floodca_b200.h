@@ -366,11 +366,15 @@ FCAB_API int fcab_batch_create(FcabBatch **out, FcabSim *const *members, int n,
                                void *stream);
 
 /* Runs every member to the end of its run. One launch advances every active
- * member by one step, in graphs of graph_steps launches. window_s > 0 paces
- * the members by output windows: replays continue until every member reaches
- * the end of the current window (window_s seconds of simulated time past the
- * previous one; steps land on window ends when out_every divides window_s),
- * then the next window opens; max_windows > 0 stops after that many windows.
+ * member by one step. Each output window is one CUDA graph launch: the graph
+ * opens the window and loops on the device (a conditional while node, passes
+ * of graph_steps steps) until no member is active, so the host waits only at
+ * window ends; without conditional graph support the host replays graphs of
+ * graph_steps steps instead. window_s > 0 paces the members by output
+ * windows: a window lasts until every member reaches its end (window_s
+ * seconds of simulated time past the previous one; steps land on window ends
+ * when out_every divides window_s), then the next window opens; max_windows
+ * > 0 stops after that many windows.
  * window_s <= 0 runs every member freely to its end. Pacing never changes a
  * member's steps: they are those of its own session run alone. Members with
  * forcing days or progress pauses are refused at fcab_batch_create. Member

@@ -140,7 +140,7 @@ class FcabInfo(C.Structure):
     _fields_ = [("cols_per_lane", C.c_int), ("grid", C.c_int), ("warps", C.c_int),
                 ("ctas_per_sm", C.c_int), ("rain_field", C.c_int), ("land_only", C.c_int),
                 ("land_cells", C.c_longlong), ("faces_per_step", C.c_longlong),
-                ("pitch", C.c_longlong)]
+                ("pitch", C.c_longlong), ("tma_rows", C.c_int)]
 
 
 class FcabBatchInfo(C.Structure):

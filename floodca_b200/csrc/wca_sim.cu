@@ -1032,6 +1032,7 @@ extern "C" int fcab_sim_info(FcabSim *s, FcabInfo *info)
     info->land_cells = s->land_cells;
     info->faces_per_step = s->faces_per_step;
     info->pitch = s->pitch;
+    info->tma_rows = s->use_tma && s->L.tma_smem > 0 ? 1 : 0;
     return 0;
 }
 

@@ -220,6 +220,7 @@ typedef struct FcabPoll {
 typedef struct FcabInfo {
     int cols_per_lane, grid, warps, ctas_per_sm, rain_field, land_only;
     long long land_cells, faces_per_step, pitch;
+    int tma_rows;             /* 1: the pair sweep reads rows by TMA (FCAB_ROW_SOURCE=tma) */
 } FcabInfo;
 
 typedef struct FcabSim FcabSim;

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from floodca_b200 import synth
-from floodca_b200.sim import run_session
+from floodca_b200.sim import Session, run_session
 from oracle import pyoracle
 
 pytestmark = pytest.mark.gpu
@@ -49,12 +49,32 @@ def test_config3_shape_precision_variants():
     assert _diff(rall["hmax"], r64["hmax"]) < 1e-2
 
 
-def test_fast_math_within_tolerance():
+@pytest.mark.parametrize("cpl", [1, 2, 4])
+def test_fast_math_within_tolerance(cpl):
+    """Hardware approximations against the exact run, on the scalar sweep
+    (one column per lane) and the packed sweeps (two and four)."""
     d, p = synth.config1()
-    ex = run_session(d, p, precision="f32", math="exact")
-    fa = run_session(d, p, precision="f32", math="fast")
+    ex = run_session(d, p, precision="f32", math="exact", cols_per_lane=cpl)
+    fa = run_session(d, p, precision="f32", math="fast", cols_per_lane=cpl)
     assert _diff(ex["hmax"], fa["hmax"]) <= 1e-3
     assert abs(ex["V"] - fa["V"]) / ex["V"] <= 1e-5
+
+
+def test_tma_row_source_equals_reference(monkeypatch):
+    """The pair sweep's TMA row source (FCAB_ROW_SOURCE=tma: z, h, n rows
+    through a shared-memory ring filled by cp.async.bulk.tensor) gives the
+    reference core's results bit for bit, like the plain loads."""
+    from floodca_b200.profile_step import warm_config2
+    from tests import refpin
+    d, p = warm_config2(512)
+    p = p.with_(steps=120)
+    monkeypatch.setenv("FCAB_ROW_SOURCE", "tma")
+    with Session(d, p, precision="f32", cols_per_lane=2) as s:
+        assert s.info()["tma_rows"] == 1
+        s.run()
+        st = s.stats()
+        h, hmax, tmax = s.download()
+    refpin.check_reference({"h": h, "hmax": hmax, "tmax": tmax, **st}, d, p)
 
 
 def test_config2_full_size_properties():

@@ -60,6 +60,22 @@ def test_fast_math_within_tolerance(cpl):
     assert abs(ex["V"] - fa["V"]) / ex["V"] <= 1e-5
 
 
+@pytest.mark.parametrize("cpl", [2, 4])
+def test_fp32_everywhere_packed_sweeps_equal_scalar(cpl):
+    """FP32-everywhere (float time and volume accumulators) on the packed
+    sweeps equals the scalar sweep in the same precision: depths, maxima,
+    times and steps bit for bit, volumes within float rounding (the
+    accumulation order differs)."""
+    d, p = synth.config1()
+    r1 = run_session(d, p, precision="f32all", cols_per_lane=1)
+    rp = run_session(d, p, precision="f32all", cols_per_lane=cpl)
+    assert rp["step"] == r1["step"] and rp["t"] == r1["t"]
+    for k in ("h", "hmax", "tmax"):
+        assert np.array_equal(rp[k], r1[k]), k
+    for k in ("V", "V_rain", "V_bnd"):
+        assert rp[k] == pytest.approx(r1[k], rel=1e-4, abs=1e-3), k
+
+
 def test_tma_row_source_equals_reference(monkeypatch):
     """The pair sweep's TMA row source (FCAB_ROW_SOURCE=tma: z, h, n rows
     through a shared-memory ring filled by cp.async.bulk.tensor) gives the

@@ -174,8 +174,11 @@ def screen(model, X, passes: int = 8, area_thr_cells: int | None = None,
     """Surrogate pass over every member: per member the predicted area above
     0.3 m (cells) and the spread (mean over the predicted wet cells, > 0.1
     m, of the MC-dropout standard deviation). Returns the flags of members
-    to re-run, the mean prediction and the timing."""
+    to re-run, the mean prediction and the timing (set-up excluded: one
+    untimed forward pass at the screening batch size first, as the CA
+    ensembles' session set-up is outside their timing)."""
     import torch
+    model.forward(X[:batch].contiguous(), dropout_seed=1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     mean, std = predict_mc(model, X, passes, batch=batch)

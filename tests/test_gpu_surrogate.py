@@ -5,11 +5,11 @@ U-Net is trained on 1000 CA runs of 128 x 128 members (same generator, 8 h
 simulated), then 2000 new members are screened (8 MC-dropout passes; members
 with a large predicted flood area or a large spread are re-run in the CA).
 Stated accuracy of the screened ensemble against the CA at this size: RMSE
-of peak depth <= 0.15 m and CSI at 0.1 m >= 0.70 (measured on a B200: 0.113 m
-and 0.741); its members/hour must be at least 1.5x the plain CA ensemble's,
-the same batched CA on every member (measured: 2.75x).
+of peak depth <= 0.15 m and CSI at 0.1 m >= 0.70 (measured on a B200: 0.112 m
+and 0.740); its members/hour must be at least 1.5x the plain CA ensemble's,
+the same batched CA on every member (measured: 2.54x).
 The full-size run (256 x 256, 2000 training runs, 10,000 members) reaches
-RMSE 0.080 m, CSI 0.837 at 3.75x."""
+RMSE 0.080 m, CSI 0.838 at 3.50x."""
 import numpy as np
 import pytest
 

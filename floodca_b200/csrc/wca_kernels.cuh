@@ -1202,11 +1202,13 @@ __host__ __device__ constexpr int step_min_blocks()
                             : CPL == 2 ? (MATH == MATH_EXACT && K == 4 ? 16 : 12) : 8)) /
            (step_threads<CPL, MATH>() / 32);
 }
-// Resident warps per SM the pair sweep's register allocation aims for (168
-// registers at 12). Measured at 4096^2 on a B200 (one-row loop): 12 warps
-// 33.9 Gcell/s against 26.0 at 8 (255 registers, no spills).
+// Resident warps per SM the pair sweep's register allocation aims for.
+// Measured at 4096^2 on a B200 (one-row loop, same box): 16 warps (128
+// registers, about 160 B of spill stores) 44.4-45.1 Gcell/s, 12 warps (160
+// registers, no spills) 41.2-41.4, 20 warps (96 registers, 532 B of
+// spills) 37.4, 8 warps 30.5-31.3: occupancy outweighs the spills up to 16.
 #ifndef FCAB_PAIR_WARPS
-#define FCAB_PAIR_WARPS 12
+#define FCAB_PAIR_WARPS 16
 #endif
 // K = 8 holds twice the face state: 8 warps (up to 255 registers, no spills)
 #ifndef FCAB_PAIR_WARPS_K8
@@ -1216,6 +1218,17 @@ template <int K>
 __host__ __device__ constexpr int pair_warps()
 {
     return K == 8 ? FCAB_PAIR_WARPS_K8 : FCAB_PAIR_WARPS;
+}
+// The batched step keeps a member descriptor and step constants per warp
+// besides the sweep state: at 16 warps (128 registers) its config-4
+// ensemble ran 44.7 G cell-steps/s against 48.2 at 12 warps, so it keeps 12.
+#ifndef FCAB_PAIR_WARPS_BATCH
+#define FCAB_PAIR_WARPS_BATCH 12
+#endif
+template <int K>
+__host__ __device__ constexpr int pair_warps_batch()
+{
+    return K == 8 ? FCAB_PAIR_WARPS_K8 : FCAB_PAIR_WARPS_BATCH;
 }
 // Resident warps per SM of the four-column sweep (twice the pair sweep's
 // state per lane: up to 255 registers at 8 warps)
@@ -1372,7 +1385,7 @@ struct BatchQ {
 };
 
 template <typename T, typename AccT, int K, int CPL, int MATH, bool RAINF, bool LANDONLY>
-__global__ void __launch_bounds__(128, use_pair_sweep<T, K, CPL, LANDONLY>() ? pair_warps<K>() / 4
+__global__ void __launch_bounds__(128, use_pair_sweep<T, K, CPL, LANDONLY>() ? pair_warps_batch<K>() / 4
                                                                       : (CPL == 2 ? 4 : 1))
 k_step_batch(const MemberD<T> *members,
                                                     const int *unit_member, int total_units,

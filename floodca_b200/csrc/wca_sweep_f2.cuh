@@ -311,7 +311,7 @@ struct PairRing {
     f2 E[4], W[4];                      // K = 8: SE (r,c)->(r+1,c+1), SW (r,c+1)->(r+1,c)
     f2 s[4];                            // limiter
     f2 Qy[4], Qe[4], Qw[4];             // scaled y / SE / SW discharges, by the upper row
-    f2 hn[4], Ln[4], n6[4];             // new depth, new level (NaN outside the grid), n^6
+    f2 Ln[4];                           // new level (NaN outside the grid)
     f2 cr[4];                           // rain field
     f2 qo[4];                           // open-edge discharge of edge cells
     unsigned ko[4];                     // open sides of the two cells (4 bits each)
@@ -362,7 +362,7 @@ __device__ __forceinline__ void rotate_ring2(PairRing<K> &R)
 {
     rot4x2(R.z); rot4x2(R.h); rot4x2(R.n); rot4x2(R.L);
     rot4x2(R.X); rot4x2(R.Y);
-    rot4x2(R.s); rot4x2(R.Qy); rot4x2(R.hn); rot4x2(R.Ln); rot4x2(R.n6);
+    rot4x2(R.s); rot4x2(R.Qy); rot4x2(R.Ln);
     rot4x2(R.cr); rot4x2(R.qo); rot4x2(R.ko); rot4x2(R.ef);
     if constexpr (K == 8) {
         rot4x2(R.zr); rot4x2(R.hr); rot4x2(R.nr); rot4x2(R.Lr);
@@ -375,7 +375,7 @@ __device__ __forceinline__ void rotate_ring(PairRing<K> &R)
 {
     rot4(R.z); rot4(R.h); rot4(R.n); rot4(R.L);
     rot4(R.X); rot4(R.Y);
-    rot4(R.s); rot4(R.Qy); rot4(R.hn); rot4(R.Ln); rot4(R.n6);
+    rot4(R.s); rot4(R.Qy); rot4(R.Ln);
     rot4(R.cr); rot4(R.qo); rot4(R.ko); rot4(R.ef);
     if constexpr (K == 8) {
         rot4(R.zr); rot4(R.hr); rot4(R.nr); rot4(R.Lr);
@@ -736,7 +736,6 @@ struct PairSweep {
                 hkeep = sel2(in0, in1, hu, R.h[Sm2]);
             }
             R.Ln[Sm2] = Ln;
-            R.hn[Sm2] = hu;
             // stage-E candidates: wet output cells whose critical velocity
             // sqrt(g h) may exceed the warp's threshold (margin 1e-6)
             unsigned ef = 0u;
@@ -747,10 +746,6 @@ struct PairSweep {
                     ef |= 1u;
                 if (cell1 && hi2(hu) >= c.tau_h && !(t && hi2(gh) <= G.thr2c))
                     ef |= 2u;
-            }
-            {
-                const f2 n2 = mul2(R.n[Sm2], R.n[Sm2]);
-                R.n6[Sm2] = mul2(mul2(n2, n2), n2);
             }
             R.ef[Sm2] = ef;
             // hmax / tmax of output cells
@@ -800,20 +795,26 @@ struct PairSweep {
                     }
                 }
             }
-            // bound: v^6 <= h^4 S^3 / n^6 (S = the largest slope), against thr^6
+            // bound: v^6 <= h^4 S^3 / n^6 (S = the largest slope), against thr^6.
+            // n and the new depth are read here, in the rare body, rather
+            // than carried in the ring through every row: a candidate is an
+            // output cell, whose new depth this thread stored in stage D of
+            // the previous row (the coherent load sees it); other lanes load
+            // nothing
+            const int off3 = G.o1 - 5 * pitch;                  // row i-3
+            const unsigned ef = R.ef[Sm3];
+            const f2 n3 = ld2(G.gn + off3);
+            const f2 n2 = mul2(n3, n3);
             f2 S = mul2(mo, c.rdx);
             if constexpr (K == 8)
                 S = max2(S, mul2(md, c.rdd));
-            const f2 hv = R.hn[Sm3];
+            const f2 hv = ef != 0u ? ld2_rw(G.hout + off3) : z0;
             const f2 h2 = mul2(hv, hv);
             const f2 lhs = mul2(mul2(h2, h2), mul2(mul2(S, S), S));
-            const f2 rhs = mul2(R.n6[Sm3], bc2(G.T6));
-            const unsigned ef = R.ef[Sm3];
+            const f2 rhs = mul2(mul2(mul2(n2, n2), n2), bc2(G.T6));
             const bool x0 = (ef & 1u) && (lo2(lhs) >= lo2(rhs) || lo2(lhs) < 1e-30f);
             const bool x1 = (ef & 2u) && (hi2(lhs) >= hi2(rhs) || hi2(lhs) < 1e-30f);
             if (__any_sync(0xffffffffu, x0 || x1)) {
-                const int off3 = G.o1 - 5 * pitch;              // row i-3
-                const f2 n3 = ld2(G.gn + off3);
                 float vm = ss.vmax;
                 if (x0 || x1)
                     vm = pair_velocity<K, MATH>(vm, x0, x1, mo, md, hv, n3, kp);
@@ -909,7 +910,7 @@ struct PairSweep {
             R.X[q] = R.Y[q] = R.E[q] = R.W[q] = z0;
             R.s[q] = bc2(1.0f);
             R.Qy[q] = R.Qe[q] = R.Qw[q] = z0;
-            R.hn[q] = R.n6[q] = R.cr[q] = R.qo[q] = z0;
+            R.cr[q] = R.qo[q] = z0;
             R.Ln[q] = bc2(__int_as_float(0x7fc00000));
             R.ko[q] = R.ef[q] = 0u;
         }

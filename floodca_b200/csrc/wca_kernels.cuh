@@ -1220,10 +1220,12 @@ __host__ __device__ constexpr int pair_warps()
     return K == 8 ? FCAB_PAIR_WARPS_K8 : FCAB_PAIR_WARPS;
 }
 // The batched step keeps a member descriptor and step constants per warp
-// besides the sweep state: at 16 warps (128 registers) its config-4
-// ensemble ran 44.7 G cell-steps/s against 48.2 at 12 warps, so it keeps 12.
+// besides the sweep state. With stage E's depth and n and the hmax row out
+// of the register ring it spills 108 B at 16 warps (128 registers), and the
+// config-4 ensemble (256 members) ran 50.9 G cell-steps/s against 48.8 at
+// 12 warps (168 registers, no spills) on one box.
 #ifndef FCAB_PAIR_WARPS_BATCH
-#define FCAB_PAIR_WARPS_BATCH 12
+#define FCAB_PAIR_WARPS_BATCH 16
 #endif
 template <int K>
 __host__ __device__ constexpr int pair_warps_batch()
